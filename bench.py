@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Throughput of the B200 spectral PFC step (Mcell-steps/s).
+
+Workload: plain conserved PFC at 512^3 on one B200, FP32 bulk arithmetic with
+FP64 operator tables / k = 0 mode (dx = pi/4, dt = 0.5, r = -0.25, psi0 =
+-0.285 + U(-0.01, 0.01), seed 7: the 512^3 case of the "256^3 and 512^3"
+configuration).  A step is one PFC time step over the whole grid with the
+state resident in HBM.  Every array (0.54 GB each) is larger than the 126 MB
+L2, so no flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+With N > 1 (torchrun, one rank per GPU) every rank evolves its own independent
+512^3 field (replicas: a single field's FFT does not shard without an all-to-all,
+and the path has none); value = all cells of all ranks * K / max-over-ranks time.
+
+--impl reference times the reference algorithm's CPU implementation on this
+host's cores instead: the FP64 C restatement of the reference path (the
+reference's own FFTW/HeFFTe/MPI build cannot be built here), same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N = 512
+DX = [math.pi / 4] * 3
+DT, R, N0, AMP, SEED = 0.5, -0.25, -0.285, 0.01, 7
+METRIC = "Mcell-steps/s at 512^3 FP32 vs FP64 GPU (<=1e-5 rel-L2); FFT-pass HBM % of peak"
+WORKLOAD = "plain conserved PFC 512^3, FP32 bulk / FP64 tables, dx=pi/4 dt=0.5 r=-0.25"
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.device), "-lms", "100"],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.p:
+            time.sleep(0.25)
+            self.p.terminate()
+            try:
+                out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+                out = ""
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def alg_bytes_per_kernel(n, prec_bytes):
+    """Algorithmic HBM bytes per launch of each kernel of the plain step."""
+    nc = (n // 2 + 1) * n * n
+    sc, st = 2 * prec_bytes, prec_bytes
+    return {"y_inverse": 2 * nc * sc, "x_fused": 2 * nc * sc, "y_forward": 2 * nc * sc,
+            "z_update": nc * (4 * sc + 2 * st), "hermitian_fix": 4 * 2 * n * n * sc}
+
+
+def cpu_baseline(psi0, budget_s=30.0):
+    """Time the FP64 C restatement of the reference step on all host threads."""
+    from oracle import oracle as O
+    threads = O.get_threads()
+    psi = np.ascontiguousarray(psi0, dtype=np.float64).copy()
+    t1 = O.time_plain(psi, DX, R, DT, 1)
+    steps, total = 1, t1
+    if t1 * 2 < budget_s:
+        k = max(1, min(5, int((budget_s - t1) / max(t1, 1e-9))))
+        total = O.time_plain(psi, DX, R, DT, k)
+        steps = k
+    cells = psi.size
+    return {"value": cells * steps / total / 1e6, "unit": "Mcell-steps/s", "cores": threads,
+            "kind": "port",
+            "sample": f"{steps} plain PFC step(s) at {N}^3 FP64 (C restatement of the reference "
+                      f"path, OpenMP {threads} threads), {total:.2f} s"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist()
+    if rank != 0:
+        return 0
+    import ctypes  # noqa: F401
+    from oracle import oracle as O
+    import openpfc_b200 as ob
+    psi = ob.ic_noise((N, N, N), N0, AMP, SEED)
+    threads = O.get_threads()
+    # bounded sample: one untimed step when affordable, then as many of the
+    # requested steps as fit in ~150 s
+    t1 = O.time_plain(psi, DX, R, DT, 1)
+    k = max(1, min(args.steps, int(150.0 / max(t1, 1e-9))))
+    t = O.time_plain(psi, DX, R, DT, k)
+    v = psi.size * k / t / 1e6
+    line = {"metric": METRIC, "value": v, "unit": "Mcell-steps/s", "n_gpus": args.gpus,
+            "steps": k, "warmup": 1, "ms_per_step": 1e3 * t / k, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD.replace("FP32 bulk / FP64 tables", "FP64 CPU"),
+                       "n": N, "l2": "arrays larger than L2"},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "Mcell-steps/s", "cores": threads, "kind": "port",
+                             "sample": f"{k} plain PFC steps at {N}^3 FP64, C restatement of the "
+                                       f"reference path (FFTW/HeFFTe/MPI absent), {threads} threads"},
+            "e2e": {"value": v, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def timed_steps(model, steps, warmup, ws, stream):
+    import torch
+    model.step(warmup)
+    model.sync()
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    model.step(steps)
+    e1.record(stream)
+    e1.synchronize()
+    model.sync()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    if ws > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    return ms
+
+
+def run_b200(args):
+    import torch
+    import openpfc_b200 as ob
+    ws, rank, local = dist()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    hbm, peak_kind = peaks()
+    cells = N ** 3
+    psi0 = ob.ic_noise((N, N, N), N0, AMP, SEED + rank)
+    psi0_32 = psi0.astype(np.float32)
+
+    m = ob.PfcB200((N, N, N), DX, r=R, precision=ob.FP32, device=local)
+    m.initialize(DT)
+    m.set_psi(psi0_32)
+    stream = torch.cuda.ExternalStream(m.stream, device=torch.device("cuda", local))
+    with Clocks(local) as ck:
+        ms = timed_steps(m, args.steps, args.warmup, ws, stream)
+    value = ws * cells * args.steps / (ms / 1e3) / 1e6
+    kps = m.kernels_per_step()
+
+    extra = {}
+    # FP64 step (same workload) and FP32-vs-FP64 accuracy after 100 steps
+    if not args.no_fp64:
+        m64 = ob.PfcB200((N, N, N), DX, r=R, precision=ob.FP64, device=local)
+        m64.initialize(DT)
+        m64.set_psi(psi0_32.astype(np.float64))
+        s64 = max(3, min(args.steps, 20))
+        ms64 = timed_steps(m64, s64, min(args.warmup, 3), ws, torch.cuda.ExternalStream(
+            m64.stream, device=torch.device("cuda", local)))
+        v64 = ws * cells * s64 / (ms64 / 1e3) / 1e6
+        extra["fp64"] = {"value": v64, "ms_per_step": ms64 / s64, "steps": s64}
+        extra["fp32_over_fp64"] = value / v64
+        if rank == 0:
+            acc_steps = 100
+            m.set_psi(psi0_32)
+            m64.set_psi(psi0_32.astype(np.float64))
+            m.step(acc_steps)
+            m64.step(acc_steps)
+            m.sync()
+            m64.sync()
+            a = m.get_psi()
+            b = m64.get_psi()
+            extra["rel_l2_fp32_vs_fp64"] = float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+            extra["rel_l2_steps"] = acc_steps
+            del a, b
+        del m64
+
+    # e2e through the public API with host buffers: per step the field goes
+    # host -> device (set_psi), one step, device -> host (get_psi), pinned memory
+    e2e = None
+    if not args.no_e2e:
+        host_in = torch.from_numpy(psi0_32.copy()).pin_memory()
+        host_out = torch.empty_like(host_in).pin_memory()
+        hin, hout = host_in.numpy(), host_out.numpy()
+        k_e2e = max(2, min(args.steps, 5))
+        m.set_psi(hin)
+        m.step(1)
+        m.get_psi(hout)
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(k_e2e):
+            m.set_psi(hin)
+            m.step(1)
+            m.get_psi(hout)
+        torch.cuda.synchronize()
+        t_e2e = time.perf_counter() - t0
+        if ws > 1:
+            t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        e2e = {"value": ws * cells * k_e2e / t_e2e / 1e6, "unit": "Mcell-steps/s",
+               "h2d_bytes_per_step": host_in.numel() * 4, "d2h_bytes_per_step": host_out.numel() * 4,
+               "steps": k_e2e, "api": "opfc_set_psi(host) + opfc_step(1) + opfc_get_psi(host)"}
+
+    # per-kernel device time (each kernel alone, CUDA events on the handle's stream)
+    m.set_psi(psi0_32)
+    prof = m.profile_step(reps=args.profile_reps)
+    ab = alg_bytes_per_kernel(N, 4)
+    passes = {}
+    for k, t in prof.items():
+        gbs = ab[k] / (t / 1e3) / 1e9
+        passes[k] = {"ms": t, "alg_bytes": ab[k], "gbs": gbs, "frac": gbs / hbm}
+    dom = max(prof, key=lambda k: prof[k])
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic_512.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(dom)
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": passes[dom]["gbs"], "peak": hbm,
+                "peak_kind": peak_kind, "unit": "GB/s", "frac": passes[dom]["frac"],
+                "traffic": traffic, "alg_bytes": ab[dom]}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(psi0)
+
+    if ws > 1:
+        torch.distributed.barrier()
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Mcell-steps/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": WORKLOAD, "n": N, "per_gpu_cells": cells,
+                           "l2": "inputs larger than L2 (0.54 GB arrays), no flush",
+                           "parallelism": f"replicas x{ws}"},
+                "e2e": e2e, "roofline": roofline, "passes": passes, "cpu_baseline": cpu,
+                "clocks": ck.summary(), "gpu_launches": kps * args.steps}
+        line.update(extra)
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-reps", type=int, default=10)
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

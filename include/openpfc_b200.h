@@ -1,0 +1,168 @@
+/*
+ * openpfc_b200.h -- C ABI of the B200-native spectral PFC time step.
+ *
+ * One handle = one periodic 3D field on one GPU.  The state is kept resident
+ * in k-space; every call returns an int status (0 = OK, negative = error) and
+ * never throws.  opfc_last_error() returns a message for the last failure on a
+ * handle.  Handles are not thread-safe; all work of a handle is issued on one
+ * CUDA stream.
+ *
+ * Layout at the boundary (identical to the reference):
+ *   real field  : N0*N1*N2 values, x fastest, idx = i + N0*(j + N1*k)
+ *                 (include/openpfc/kernel/field/operations.hpp:96-103)
+ *   half spectrum: (N0/2+1)*N1*N2 complex values, interleaved (re, im), same
+ *                 order (src/openpfc/runtime/cpu/fft.cpp:58-70)
+ *   forward transform unnormalised, backward scaled by 1/(N0*N1*N2)
+ *                 (include/openpfc/kernel/fft/detail/fft_heffte_backend.hpp:216,243)
+ */
+#ifndef OPENPFC_B200_H
+#define OPENPFC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define OPFC_OK 0
+#define OPFC_ERR_ARG (-1)         /* bad argument (null pointer, bad enum)      */
+#define OPFC_ERR_SIZE (-2)        /* size contract violated / unsupported size  */
+#define OPFC_ERR_CUDA (-3)        /* CUDA runtime error                         */
+#define OPFC_ERR_NONFINITE (-4)   /* NaN/Inf detected in the field              */
+#define OPFC_ERR_TIMEOUT (-5)     /* bounded device wait expired                */
+#define OPFC_ERR_OOM (-6)         /* device allocation failed                   */
+#define OPFC_ERR_STATE (-7)       /* call out of order (e.g. step before init)  */
+
+/* precision of the bulk arithmetic */
+#define OPFC_FP32 0
+#define OPFC_FP64 1
+
+/* model kinds */
+#define OPFC_MODEL_PLAIN 0     /* conserved PFC, docs/api/examples/10_complete_pfc_model.cpp:121-213 */
+#define OPFC_MODEL_TUNGSTEN 1  /* Tungsten ETD, apps/tungsten/include/tungsten/cpu/tungsten_model.hpp:306-366 */
+#define OPFC_MODEL_FILTERED 2  /* Gaussian mean-field filter + polynomial of psi_MF */
+
+/* where a user pointer lives */
+#define OPFC_HOST 0
+#define OPFC_DEVICE 1
+
+/* element type of a user buffer */
+#define OPFC_F32 0
+#define OPFC_F64 1
+
+/* Tungsten base parameters, same names and defaults as
+ * apps/tungsten/include/tungsten/common/tungsten_params.hpp:33-57. */
+typedef struct opfc_tungsten_params {
+  double n0, n_sol, n_vap, T, T0, Bx, alpha, alpha_farTol;
+  int alpha_highOrd;
+  double lambda, stabP, shift_u, shift_s, p2, p3, p4, q20, q21, q30, q31, q40;
+} opfc_tungsten_params;
+
+typedef struct opfc_desc {
+  int n[3];            /* N0 (x, fastest), N1, N2 */
+  double dx[3];        /* grid spacing */
+  double origin[3];    /* physical coordinate of cell (0,0,0) */
+  int precision;       /* OPFC_FP32 / OPFC_FP64 */
+  int model;           /* OPFC_MODEL_* */
+  double r;            /* PLAIN/FILTERED: L(k) = -k^2 (r + (1-k^2)^2) */
+  double filter_alpha; /* FILTERED: chi = exp(-k^2 / (2 alpha^2)) */
+  double p2, p3, p4;   /* FILTERED: N = p2 v^2/2 + p3 v^3/3 + p4 v^4/4, v = psi_MF */
+  opfc_tungsten_params tungsten; /* TUNGSTEN */
+  void *stream;        /* cudaStream_t to use, or NULL for a private stream */
+  int device;          /* CUDA device ordinal */
+} opfc_desc;
+
+typedef struct opfc_handle opfc_handle;
+
+/* Fill a descriptor with defaults: TungstenParams defaults, dx = 1,
+ * origin = 0, FP32, PLAIN, r = -0.25.  Replaces the default-constructed
+ * parameter block of tungsten_params.hpp:33-57. */
+void opfc_desc_default(opfc_desc *desc);
+
+/* Lifetime.  opfc_create replaces the GPU model ctor + FFT plan
+ * (apps/tungsten/include/tungsten/cuda/tungsten_model.hpp:132-178). */
+int opfc_create(const opfc_desc *desc, opfc_handle **out);
+int opfc_destroy(opfc_handle *h);
+const char *opfc_last_error(const opfc_handle *h);
+const char *opfc_status_string(int status);
+
+/* Operator tables in FP64 on the host, rounded to the handle precision and
+ * uploaded.  Replaces Model::initialize(dt) / prepare_operators
+ * (cpu/tungsten_model.hpp:223-292; 10_complete_pfc_model.cpp:94-115,166-213). */
+int opfc_initialize(opfc_handle *h, double dt);
+
+/* Field access.  count must be N0*N1*N2 (real) or (N0/2+1)*N1*N2 (complex);
+ * dtype OPFC_F32/OPFC_F64; where OPFC_HOST/OPFC_DEVICE (device pointers must
+ * hold the handle's own precision).  set_psi replaces writing the registered
+ * "psi" field + finalize_after_field_modifiers (model.hpp:272); get_psi
+ * replaces prepare_for_field_modifiers (model.hpp:265) + reading "psi". */
+int opfc_set_psi(opfc_handle *h, const void *psi, size_t count, int dtype, int where);
+int opfc_get_psi(opfc_handle *h, void *psi, size_t count, int dtype, int where);
+int opfc_get_psi_hat(opfc_handle *h, void *psi_hat, size_t count, int dtype, int where);
+/* The mean-field filtered density psi_MF (Tungsten "psiMF" field,
+ * cpu/tungsten_model.hpp:200), computed from the current state. */
+int opfc_get_psi_mf(opfc_handle *h, void *psi_mf, size_t count, int dtype, int where);
+
+/* Advance n_steps time steps (Model::step, cpu/tungsten_model.hpp:306;
+ * 10_complete_pfc_model.cpp:121).  Asynchronous on the handle's stream; the
+ * step sequence is captured in a CUDA graph on first use. */
+int opfc_step(opfc_handle *h, int n_steps);
+/* Wait for the handle's stream; reports OPFC_ERR_NONFINITE if any step
+ * produced NaN/Inf since the last check. */
+int opfc_sync(opfc_handle *h);
+
+/* Stand-alone transforms with the reference's IFFT contract
+ * (include/openpfc/kernel/fft/fft_interface.hpp:51,61): forward R2C
+ * unnormalised, backward C2R scaled by 1/(N0 N1 N2).  Buffers as above. */
+int opfc_fft_forward(opfc_handle *h, const void *in_real, void *out_complex, int dtype, int where);
+int opfc_fft_backward(opfc_handle *h, const void *in_complex, void *out_real, int dtype, int where);
+
+/* Diagnostics.  mass = mean density (sum psi / N0 N1 N2), carried in FP64.
+ * free energy (plain / filtered models; project-defined, the reference has
+ * none): F = sum dV [1/2 psi F^-1{(r + (1-k^2)^2) psi_hat} + 1/4 psi^4],
+ * reduced in FP64. */
+int opfc_mass(opfc_handle *h, double *mean_density);
+int opfc_free_energy(opfc_handle *h, double *energy);
+
+/* Introspection (IFFT::size_inbox/size_outbox/get_allocated_memory_bytes,
+ * fft_interface.hpp:68-72). */
+size_t opfc_size_inbox(const opfc_handle *h);
+size_t opfc_size_outbox(const opfc_handle *h);
+size_t opfc_allocated_bytes(const opfc_handle *h);
+void *opfc_get_stream(const opfc_handle *h);
+/* Number of kernels one opfc_step(1) launches (for launch accounting). */
+int opfc_kernels_per_step(const opfc_handle *h);
+/* Measurement hook (no reference counterpart; the reference times FFT calls
+ * with MPI_Wtime, fft_heffte_backend.hpp:158-164): times each kernel of the
+ * step alone, `reps` launches each, with CUDA events on the handle's stream;
+ * ms[k] = mean milliseconds per launch.  Returns the number of kernels timed
+ * (>= 0) or an error.  The repeated in-place passes leave the field undefined:
+ * call opfc_set_psi before stepping again. */
+int opfc_profile_step(opfc_handle *h, int reps, double *ms, int max_kernels);
+/* Name of kernel k of the step ("y_inverse", "x_fused", ...). */
+const char *opfc_step_kernel_name(int k);
+
+/* Initial conditions, host-side (set-up only), x-fastest cell order.
+ * Random numbers: one draw of std::mt19937_64(seed) per number, mapped to
+ * [0,1) as (draw >> 11) * 2^-53.
+ * opfc_ic_noise: psi = n0 + U(-amp, amp) per cell.
+ * opfc_ic_seed: one-mode BCC seed, u = rho + sum_q 2 amp cos(q.(x - center)) over
+ *   the six <110>/sqrt(2) vectors inside |x - center| < radius, x = origin + i dx
+ *   (include/openpfc/kernel/simulation/initial_conditions/single_seed.hpp; with
+ *   outside_zero = 1 the outside is zeroed like SingleSeed::apply, with 0 it is
+ *   left as is like apps/tungsten/tests/test_tungsten.cpp:262-280).
+ * opfc_ic_seeds: noisy liquid n0 + U(-noise, noise), then nseeds spheres of
+ *   radius_cells at centres (u0 N0, u1 N1, u2 N2) drawn from the same stream,
+ *   filled with n0 + amp sum_q cos(q.(x - c)) (periodic minimum image). */
+int opfc_ic_noise(double *psi, size_t count, double n0, double amp, uint64_t seed);
+int opfc_ic_seed(double *psi, const int n[3], const double dx[3], const double origin[3],
+                 const double center[3], double radius, double rho, double amp, int outside_zero);
+int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, double noise,
+                  int nseeds, double radius_cells, double amp, uint64_t seed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OPENPFC_B200_H */

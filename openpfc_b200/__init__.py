@@ -1,0 +1,306 @@
+"""openpfc_b200 -- B200-native spectral PFC time step behind OpenPFC's API.
+
+The compute path is libopenpfc_b200.so (hand-written sm_100a kernels, C ABI in
+include/openpfc_b200.h).  This module is the Python mirror of the reference's
+host interface for that path:
+
+  * :class:`B200Fft`   -- pfc::fft::IFFT (include/openpfc/kernel/fft/fft_interface.hpp:40-83)
+  * :class:`PfcB200`   -- the plain conserved PFC model
+                          (docs/api/examples/10_complete_pfc_model.cpp:62-214)
+  * :class:`TungstenB200` -- the Tungsten model (apps/tungsten/include/tungsten/
+                          cpu/tungsten_model.hpp:123-380), params as TungstenParams
+  * :class:`FilteredB200` -- Gaussian mean-field filter + polynomial of psi_MF
+
+Errors follow the reference: size contracts raise ValueError (the reference's
+std::invalid_argument), everything else raises RuntimeError.  Host arrays are
+numpy (x fastest: shape (N2, N1, N0)); device arrays are torch CUDA tensors.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import (DEVICE, F32, F64, FP32, FP64, HOST, MODEL_FILTERED, MODEL_PLAIN,
+                   MODEL_TUNGSTEN, Desc, OpfcError, TungstenParams, default_desc, lib)
+
+__all__ = ["B200Fft", "PfcB200", "TungstenB200", "FilteredB200", "Desc", "TungstenParams",
+           "OpfcError", "default_desc", "lib", "FP32", "FP64"]
+
+
+def _check(h, rc: int):
+    if rc != 0:
+        msg = lib().opfc_last_error(h).decode() if h else ""
+        if rc == -2:
+            raise ValueError(f"OPFC_ERR_SIZE: {msg}")
+        raise OpfcError(rc, msg)
+
+
+def _buf(arr, writable: bool = False):
+    """(pointer, count, dtype code, location) of a numpy array or torch tensor."""
+    if isinstance(arr, np.ndarray):
+        if not arr.flags.c_contiguous:
+            raise ValueError("array must be C-contiguous")
+        if arr.dtype == np.float64:
+            dt = F64
+        elif arr.dtype == np.float32:
+            dt = F32
+        else:
+            raise ValueError(f"unsupported dtype {arr.dtype}")
+        return ctypes.c_void_p(arr.ctypes.data), arr.size, dt, HOST
+    import torch  # device buffers are torch tensors
+    if isinstance(arr, torch.Tensor):
+        if not arr.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        if arr.dtype == torch.float64:
+            dt = F64
+        elif arr.dtype == torch.float32:
+            dt = F32
+        else:
+            raise ValueError(f"unsupported dtype {arr.dtype}")
+        loc = DEVICE if arr.is_cuda else HOST
+        return ctypes.c_void_p(arr.data_ptr()), arr.numel(), dt, loc
+    raise TypeError(f"unsupported buffer type {type(arr)}")
+
+
+class _Handle:
+    def __init__(self, desc: Desc):
+        self._h = ctypes.c_void_p()
+        self.desc = desc
+        _check(None, lib().opfc_create(ctypes.byref(desc), ctypes.byref(self._h)))
+        self.shape = (desc.n[2], desc.n[1], desc.n[0])
+        self.half_shape = (desc.n[2], desc.n[1], desc.n[0] // 2 + 1)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().opfc_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def size_inbox(self) -> int:
+        return int(lib().opfc_size_inbox(self._h))
+
+    def size_outbox(self) -> int:
+        return int(lib().opfc_size_outbox(self._h))
+
+    def get_allocated_memory_bytes(self) -> int:
+        return int(lib().opfc_allocated_bytes(self._h))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().opfc_get_stream(self._h) or 0)
+
+    @property
+    def real_dtype(self):
+        return np.float64 if self.desc.precision == FP64 else np.float32
+
+
+class B200Fft(_Handle):
+    """pfc::fft::IFFT on one B200: forward R2C unnormalised, backward C2R scaled
+    by 1/(N0 N1 N2) (fft_heffte_backend.hpp:216,243).  Sizes are checked like the
+    reference (fft_heffte_backend.hpp:151-156)."""
+
+    def __init__(self, n, dx=(1.0, 1.0, 1.0), precision: int = FP64, device: int = 0):
+        d = default_desc()
+        for a in range(3):
+            d.n[a] = int(n[a])
+            d.dx[a] = float(dx[a])
+        d.precision = precision
+        d.device = device
+        super().__init__(d)
+        self._fft_time = 0.0
+
+    def forward(self, inp, out=None):
+        if out is None:
+            out = np.zeros(self.half_shape, dtype=np.complex128)
+        ob = out.view(np.float64) if isinstance(out, np.ndarray) and out.dtype == np.complex128 else \
+            (out.view(np.float32) if isinstance(out, np.ndarray) and out.dtype == np.complex64 else out)
+        ip, icnt, idt, iloc = _buf(inp)
+        op, ocnt, odt, oloc = _buf(ob)
+        if icnt != self.size_inbox() or ocnt != 2 * self.size_outbox():
+            raise ValueError(f"FFT forward: expected {self.size_inbox()} reals in and "
+                             f"{self.size_outbox()} complex out, got {icnt} and {ocnt // 2}")
+        if idt != odt or iloc != oloc:
+            raise ValueError("input and output must share dtype and location")
+        _check(self._h, lib().opfc_fft_forward(self._h, ip, op, idt, iloc))
+        return out
+
+    def backward(self, inp, out=None):
+        if out is None:
+            out = np.zeros(self.shape, dtype=np.float64)
+        ib = inp.view(np.float64) if isinstance(inp, np.ndarray) and inp.dtype == np.complex128 else \
+            (inp.view(np.float32) if isinstance(inp, np.ndarray) and inp.dtype == np.complex64 else inp)
+        ip, icnt, idt, iloc = _buf(np.ascontiguousarray(ib) if isinstance(ib, np.ndarray) else ib)
+        op, ocnt, odt, oloc = _buf(out)
+        if icnt != 2 * self.size_outbox() or ocnt != self.size_inbox():
+            raise ValueError(f"FFT backward: expected {self.size_outbox()} complex in and "
+                             f"{self.size_inbox()} reals out, got {icnt // 2} and {ocnt}")
+        if idt != odt or iloc != oloc:
+            raise ValueError("input and output must share dtype and location")
+        _check(self._h, lib().opfc_fft_backward(self._h, ip, op, idt, iloc))
+        return out
+
+    def reset_fft_time(self):
+        self._fft_time = 0.0
+
+    def get_fft_time(self) -> float:
+        return self._fft_time
+
+
+class _ModelBase(_Handle):
+    def initialize(self, dt: float):
+        _check(self._h, lib().opfc_initialize(self._h, float(dt)))
+
+    def set_psi(self, psi):
+        p, cnt, dt, loc = _buf(psi)
+        _check(self._h, lib().opfc_set_psi(self._h, p, cnt, dt, loc))
+
+    def get_psi(self, out=None):
+        if out is None:
+            out = np.zeros(self.shape, dtype=np.float64)
+        p, cnt, dt, loc = _buf(out)
+        _check(self._h, lib().opfc_get_psi(self._h, p, cnt, dt, loc))
+        return out
+
+    def get_psi_mf(self, out=None):
+        if out is None:
+            out = np.zeros(self.shape, dtype=np.float64)
+        p, cnt, dt, loc = _buf(out)
+        _check(self._h, lib().opfc_get_psi_mf(self._h, p, cnt, dt, loc))
+        return out
+
+    def get_psi_hat(self, out=None):
+        if out is None:
+            out = np.zeros(self.half_shape, dtype=np.complex128)
+        ob = out.view(np.float64) if out.dtype == np.complex128 else out.view(np.float32)
+        p, cnt, dt, loc = _buf(ob)
+        _check(self._h, lib().opfc_get_psi_hat(self._h, p, cnt // 2, dt, loc))
+        return out
+
+    def step(self, n_steps: int = 1):
+        """Advance n_steps steps (asynchronous; see :meth:`sync`)."""
+        _check(self._h, lib().opfc_step(self._h, int(n_steps)))
+
+    def sync(self):
+        _check(self._h, lib().opfc_sync(self._h))
+
+    def mass(self) -> float:
+        v = ctypes.c_double()
+        _check(self._h, lib().opfc_mass(self._h, ctypes.byref(v)))
+        return v.value
+
+    def free_energy(self) -> float:
+        v = ctypes.c_double()
+        _check(self._h, lib().opfc_free_energy(self._h, ctypes.byref(v)))
+        return v.value
+
+    def kernels_per_step(self) -> int:
+        return int(lib().opfc_kernels_per_step(self._h))
+
+    def profile_step(self, reps: int = 10) -> dict:
+        """Mean ms per launch of each kernel of the step, timed alone with CUDA
+        events on the handle's stream.  Leaves the field undefined."""
+        ms = (ctypes.c_double * 8)()
+        n = lib().opfc_profile_step(self._h, int(reps), ms, 8)
+        if n < 0:
+            _check(self._h, n)
+        return {lib().opfc_step_kernel_name(k).decode(): ms[k] for k in range(n)}
+
+
+def _geom(d: Desc, n, dx, origin, precision, device, stream):
+    for a in range(3):
+        d.n[a] = int(n[a])
+        d.dx[a] = float(dx[a])
+        d.origin[a] = float(origin[a]) if origin is not None else 0.0
+    d.precision = precision
+    d.device = device
+    d.stream = stream
+
+
+class PfcB200(_ModelBase):
+    """Plain conserved PFC: L(k) = -k^2 (r + (1-k^2)^2), opL = exp(L dt),
+    opN = (opL - 1)/L (-k^2) (10_complete_pfc_model.cpp:166-213); N = psi^3."""
+
+    def __init__(self, n, dx, r: float = -0.25, precision: int = FP32, device: int = 0,
+                 origin=None, stream=None):
+        d = default_desc()
+        _geom(d, n, dx, origin, precision, device, stream)
+        d.model = MODEL_PLAIN
+        d.r = float(r)
+        super().__init__(d)
+
+
+class FilteredB200(_ModelBase):
+    """Mean-field-filtered PFC: psi_MF = F^-1[exp(-k^2/(2 alpha^2)) psi_hat],
+    N = p2 psi_MF^2/2 + p3 psi_MF^3/3 + p4 psi_MF^4/4, plain opL/opN at r."""
+
+    def __init__(self, n, dx, r=-0.3, alpha=0.5, p2=-0.1, p3=-0.5, p4=0.3,
+                 precision: int = FP32, device: int = 0, origin=None, stream=None):
+        d = default_desc()
+        _geom(d, n, dx, origin, precision, device, stream)
+        d.model = MODEL_FILTERED
+        d.r, d.filter_alpha, d.p2, d.p3, d.p4 = float(r), float(alpha), float(p2), float(p3), float(p4)
+        super().__init__(d)
+
+
+class TungstenB200(_ModelBase):
+    """Tungsten model; ``params`` is a TungstenParams (defaults of tungsten_params.hpp)."""
+
+    def __init__(self, n, dx, params: TungstenParams | None = None, precision: int = FP64,
+                 device: int = 0, origin=None, stream=None):
+        d = default_desc()
+        _geom(d, n, dx, origin, precision, device, stream)
+        d.model = MODEL_TUNGSTEN
+        if params is not None:
+            d.tungsten = params
+        super().__init__(d)
+
+
+# ---------------------------------------------------------------------------
+# initial conditions (host-side set-up, libopenpfc_b200.so)
+# ---------------------------------------------------------------------------
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _i3(v):
+    return (ctypes.c_int * 3)(*[int(x) for x in v])
+
+
+def _d3(v):
+    return (ctypes.c_double * 3)(*[float(x) for x in v])
+
+
+def ic_noise(n, n0: float, amp: float, seed: int) -> np.ndarray:
+    """psi = n0 + U(-amp, amp) per cell (x fastest), std::mt19937_64(seed)."""
+    psi = np.empty((n[2], n[1], n[0]), dtype=np.float64)
+    _check(None, lib().opfc_ic_noise(_dp(psi), psi.size, n0, amp, seed))
+    return psi
+
+
+def ic_seed(psi: np.ndarray, dx, origin, center, radius, rho, amp, outside_zero=False):
+    """One-mode BCC seed (single_seed.hpp); modifies and returns psi."""
+    n = (psi.shape[2], psi.shape[1], psi.shape[0])
+    assert psi.dtype == np.float64 and psi.flags.c_contiguous
+    _check(None, lib().opfc_ic_seed(_dp(psi), _i3(n), _d3(dx), _d3(origin), _d3(center), radius,
+                                    rho, amp, int(outside_zero)))
+    return psi
+
+
+def ic_seeds(n, dx, n0, noise, nseeds, radius_cells, amp, seed) -> np.ndarray:
+    """Noisy liquid with `nseeds` seeded BCC spheres (see opfc_ic_seeds)."""
+    psi = np.empty((n[2], n[1], n[0]), dtype=np.float64)
+    _check(None, lib().opfc_ic_seeds(_dp(psi), _i3(n), _d3(dx), n0, noise, nseeds, radius_cells,
+                                     amp, seed))
+    return psi

@@ -1,0 +1,115 @@
+"""ctypes binding of libopenpfc_b200.so (C ABI in include/openpfc_b200.h).
+
+The library is the only compute path: if it is missing or fails to load,
+every call raises -- there is no CPU or PyTorch fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libopenpfc_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "openpfc_b200.h")
+
+OPFC_OK = 0
+STATUS = {0: "OPFC_OK", -1: "OPFC_ERR_ARG", -2: "OPFC_ERR_SIZE", -3: "OPFC_ERR_CUDA",
+          -4: "OPFC_ERR_NONFINITE", -5: "OPFC_ERR_TIMEOUT", -6: "OPFC_ERR_OOM",
+          -7: "OPFC_ERR_STATE"}
+FP32, FP64 = 0, 1
+MODEL_PLAIN, MODEL_TUNGSTEN, MODEL_FILTERED = 0, 1, 2
+HOST, DEVICE = 0, 1
+F32, F64 = 0, 1
+
+
+class TungstenParams(ctypes.Structure):
+    """Mirror of opfc_tungsten_params (tungsten_params.hpp:33-57 names)."""
+    _fields_ = [("n0", ctypes.c_double), ("n_sol", ctypes.c_double),
+                ("n_vap", ctypes.c_double), ("T", ctypes.c_double),
+                ("T0", ctypes.c_double), ("Bx", ctypes.c_double),
+                ("alpha", ctypes.c_double), ("alpha_farTol", ctypes.c_double),
+                ("alpha_highOrd", ctypes.c_int), ("lambda_", ctypes.c_double),
+                ("stabP", ctypes.c_double), ("shift_u", ctypes.c_double),
+                ("shift_s", ctypes.c_double), ("p2", ctypes.c_double),
+                ("p3", ctypes.c_double), ("p4", ctypes.c_double),
+                ("q20", ctypes.c_double), ("q21", ctypes.c_double),
+                ("q30", ctypes.c_double), ("q31", ctypes.c_double),
+                ("q40", ctypes.c_double)]
+
+
+class Desc(ctypes.Structure):
+    """Mirror of opfc_desc."""
+    _fields_ = [("n", ctypes.c_int * 3), ("dx", ctypes.c_double * 3),
+                ("origin", ctypes.c_double * 3), ("precision", ctypes.c_int),
+                ("model", ctypes.c_int), ("r", ctypes.c_double),
+                ("filter_alpha", ctypes.c_double), ("p2", ctypes.c_double),
+                ("p3", ctypes.c_double), ("p4", ctypes.c_double),
+                ("tungsten", TungstenParams), ("stream", ctypes.c_void_p),
+                ("device", ctypes.c_int)]
+
+
+class OpfcError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def declared_symbols() -> list[str]:
+    """Every function the public header declares."""
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(opfc_[a-z0-9_]+)\s*\(", txt)))
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError(f"{LIB_PATH} is missing: build it with `python -m openpfc_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    H = ctypes.c_void_p
+    vp, sz, ci, cd = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int, ctypes.c_double
+    L.opfc_desc_default.argtypes = [ctypes.POINTER(Desc)]
+    L.opfc_desc_default.restype = None
+    L.opfc_create.argtypes = [ctypes.POINTER(Desc), ctypes.POINTER(H)]
+    L.opfc_destroy.argtypes = [H]
+    L.opfc_last_error.argtypes = [H]
+    L.opfc_last_error.restype = ctypes.c_char_p
+    L.opfc_status_string.argtypes = [ci]
+    L.opfc_status_string.restype = ctypes.c_char_p
+    L.opfc_initialize.argtypes = [H, cd]
+    for name in ("opfc_set_psi",):
+        getattr(L, name).argtypes = [H, vp, sz, ci, ci]
+    for name in ("opfc_get_psi", "opfc_get_psi_hat", "opfc_get_psi_mf"):
+        getattr(L, name).argtypes = [H, vp, sz, ci, ci]
+    L.opfc_step.argtypes = [H, ci]
+    L.opfc_sync.argtypes = [H]
+    L.opfc_fft_forward.argtypes = [H, vp, vp, ci, ci]
+    L.opfc_fft_backward.argtypes = [H, vp, vp, ci, ci]
+    L.opfc_mass.argtypes = [H, ctypes.POINTER(cd)]
+    L.opfc_free_energy.argtypes = [H, ctypes.POINTER(cd)]
+    for name in ("opfc_size_inbox", "opfc_size_outbox", "opfc_allocated_bytes"):
+        getattr(L, name).argtypes = [H]
+        getattr(L, name).restype = sz
+    L.opfc_get_stream.argtypes = [H]
+    L.opfc_get_stream.restype = vp
+    L.opfc_kernels_per_step.argtypes = [H]
+    L.opfc_profile_step.argtypes = [H, ci, ctypes.POINTER(cd), ci]
+    L.opfc_step_kernel_name.argtypes = [ci]
+    L.opfc_step_kernel_name.restype = ctypes.c_char_p
+    dp, ip = ctypes.POINTER(cd), ctypes.POINTER(ci)
+    L.opfc_ic_noise.argtypes = [dp, sz, cd, cd, ctypes.c_uint64]
+    L.opfc_ic_seed.argtypes = [dp, ip, dp, dp, dp, cd, cd, cd, ci]
+    L.opfc_ic_seeds.argtypes = [dp, ip, dp, cd, cd, ci, cd, cd, ctypes.c_uint64]
+    _lib = L
+    return L
+
+
+def default_desc() -> Desc:
+    d = Desc()
+    lib().opfc_desc_default(ctypes.byref(d))
+    return d

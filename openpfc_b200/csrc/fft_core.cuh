@@ -1,0 +1,232 @@
+// fft_core.cuh -- register-resident Stockham FFT building blocks for sm_100a.
+//
+// A line of length N is owned by T = N/E threads of one CTA; each thread keeps
+// E complex values in registers.  On entry to a transform thread j holds the
+// line positions p = j + T*m (m = 0..E-1) and on exit it holds the transformed
+// values at the same positions (Stockham autosort: the first stage reads and the
+// last stage writes the "stride N/R" pattern, so nothing is permuted).  Between
+// stages the line is exchanged through shared memory laid out [p][c] with a
+// row pitch `ld` (W lines interleaved, c fastest) -- conflict-free for the
+// c-fastest thread mapping used by every kernel.
+//
+// Twiddles come from a per-CTA shared-memory table tw[i] = exp(-2 pi i i / TWS)
+// built on the host in FP64 and rounded to the compute precision; the inverse
+// direction uses the conjugate.  TWS is a multiple of N (TWS = 2N for the
+// half-length complex FFT inside a real transform of length 2N).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace opfc {
+
+template <typename R> struct Cx;
+template <> struct Cx<float> { using T = float2; };
+template <> struct Cx<double> { using T = double2; };
+
+template <typename C> __device__ __forceinline__ C mk(decltype(C::x) a, decltype(C::x) b) {
+  C r;
+  r.x = a;
+  r.y = b;
+  return r;
+}
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return mk<C>(a.x + b.x, a.y + b.y); }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return mk<C>(a.x - b.x, a.y - b.y); }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return mk<C>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mk<C>(a.x * s, a.y * s); }
+
+// a * w (DIR < 0) or a * conj(w) (DIR > 0)
+template <int DIR, typename C> __device__ __forceinline__ C twmul(C a, C w) {
+  if (DIR < 0) return mk<C>(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);
+  return mk<C>(a.x * w.x + a.y * w.y, a.y * w.x - a.x * w.y);
+}
+// a * exp(DIR * i pi / 2): -i for the forward direction, +i for the inverse
+template <int DIR, typename C> __device__ __forceinline__ C rot90(C a) {
+  return DIR < 0 ? mk<C>(a.y, -a.x) : mk<C>(-a.y, a.x);
+}
+
+// ---------------------------------------------------------------------------
+// radix-R DFT kernels on registers, sign DIR (-1 forward, +1 inverse)
+// ---------------------------------------------------------------------------
+template <int R, int DIR, typename C> struct Dft;
+
+template <int DIR, typename C> struct Dft<1, DIR, C> {
+  static __device__ __forceinline__ void run(C (&)[1]) {}
+};
+
+template <int DIR, typename C> struct Dft<2, DIR, C> {
+  static __device__ __forceinline__ void run(C (&v)[2]) {
+    C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+
+template <int DIR, typename C> struct Dft<4, DIR, C> {
+  static __device__ __forceinline__ void run4(C &v0, C &v1, C &v2, C &v3) {
+    C a = cadd(v0, v2), b = csub(v0, v2);
+    C c = cadd(v1, v3), d = rot90<DIR>(csub(v1, v3));
+    v0 = cadd(a, c);
+    v2 = csub(a, c);
+    v1 = cadd(b, d);
+    v3 = csub(b, d);
+  }
+  static __device__ __forceinline__ void run(C (&v)[4]) { run4(v[0], v[1], v[2], v[3]); }
+};
+
+template <int DIR, typename C> struct Dft<8, DIR, C> {
+  static __device__ __forceinline__ void run(C (&v)[8]) {
+    using S = decltype(C::x);
+    const S h = S(0.70710678118654752440084436210484904);
+    Dft<4, DIR, C>::run4(v[0], v[2], v[4], v[6]);
+    Dft<4, DIR, C>::run4(v[1], v[3], v[5], v[7]);
+    // twiddle the odd half by w8^k, w8 = exp(DIR * 2 pi i / 8)
+    C o1 = v[3], o2 = v[5], o3 = v[7];
+    if (DIR < 0) {
+      o1 = mk<C>(h * (o1.x + o1.y), h * (o1.y - o1.x));
+      o3 = mk<C>(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+    } else {
+      o1 = mk<C>(h * (o1.x - o1.y), h * (o1.x + o1.y));
+      o3 = mk<C>(-h * (o3.x + o3.y), h * (o3.x - o3.y));
+    }
+    o2 = rot90<DIR>(o2);
+    C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6], o0 = v[1];
+    v[0] = cadd(e0, o0);
+    v[4] = csub(e0, o0);
+    v[1] = cadd(e1, o1);
+    v[5] = csub(e1, o1);
+    v[2] = cadd(e2, o2);
+    v[6] = csub(e2, o2);
+    v[3] = cadd(e3, o3);
+    v[7] = csub(e3, o3);
+  }
+};
+
+template <int DIR, typename C> struct Dft<3, DIR, C> {
+  static __device__ __forceinline__ void run(C (&v)[3]) {
+    using S = decltype(C::x);
+    const S s3 = S(0.86602540378443864676372317075293618);
+    C a = v[0], b = v[1], c = v[2];
+    C t = cadd(b, c);
+    C m = mk<C>(a.x - S(0.5) * t.x, a.y - S(0.5) * t.y);
+    C d = csub(b, c);
+    // forward: X1 = m - i s3 d, X2 = m + i s3 d ; inverse flips the sign
+    C id = mk<C>(-s3 * d.y, s3 * d.x);  // i * s3 * d
+    v[0] = cadd(a, t);
+    if (DIR < 0) {
+      v[1] = csub(m, id);
+      v[2] = cadd(m, id);
+    } else {
+      v[1] = cadd(m, id);
+      v[2] = csub(m, id);
+    }
+  }
+};
+
+template <int DIR, typename C> struct Dft<5, DIR, C> {
+  static __device__ __forceinline__ void run(C (&v)[5]) {
+    using S = decltype(C::x);
+    const S c1 = S(0.30901699437494742410229341718281906);
+    const S c2 = S(-0.80901699437494742410229341718281906);
+    const S s1 = S(0.95105651629515357211643933337938214);
+    const S s2 = S(0.58778525229247312916870595463907277);
+    C a = v[0];
+    C be = cadd(v[1], v[4]), bm = csub(v[1], v[4]);
+    C cd = cadd(v[2], v[3]), cm = csub(v[2], v[3]);
+    C r1 = mk<C>(a.x + c1 * be.x + c2 * cd.x, a.y + c1 * be.y + c2 * cd.y);
+    C r2 = mk<C>(a.x + c2 * be.x + c1 * cd.x, a.y + c2 * be.y + c1 * cd.y);
+    // q1 = s1 bm + s2 cm ; q2 = s2 bm - s1 cm ; X1 = r1 - i q1 (forward)
+    C q1 = mk<C>(s1 * bm.x + s2 * cm.x, s1 * bm.y + s2 * cm.y);
+    C q2 = mk<C>(s2 * bm.x - s1 * cm.x, s2 * bm.y - s1 * cm.y);
+    C iq1 = mk<C>(-q1.y, q1.x), iq2 = mk<C>(-q2.y, q2.x);
+    v[0] = mk<C>(a.x + be.x + cd.x, a.y + be.y + cd.y);
+    if (DIR < 0) {
+      v[1] = csub(r1, iq1);
+      v[2] = csub(r2, iq2);
+      v[3] = cadd(r2, iq2);
+      v[4] = cadd(r1, iq1);
+    } else {
+      v[1] = cadd(r1, iq1);
+      v[2] = cadd(r2, iq2);
+      v[3] = csub(r2, iq2);
+      v[4] = csub(r1, iq1);
+    }
+  }
+};
+
+// ---------------------------------------------------------------------------
+// plans: elements per thread E and the radix sequence for each line length
+// ---------------------------------------------------------------------------
+template <int... Rs> struct Radices {};
+
+template <int N> struct Plan;
+template <> struct Plan<1> { static constexpr int E = 1; using R = Radices<>; };
+template <> struct Plan<2> { static constexpr int E = 2; using R = Radices<2>; };
+template <> struct Plan<4> { static constexpr int E = 4; using R = Radices<4>; };
+template <> struct Plan<8> { static constexpr int E = 8; using R = Radices<8>; };
+template <> struct Plan<16> { static constexpr int E = 8; using R = Radices<2, 8>; };
+template <> struct Plan<32> { static constexpr int E = 8; using R = Radices<4, 8>; };
+template <> struct Plan<64> { static constexpr int E = 8; using R = Radices<8, 8>; };
+template <> struct Plan<128> { static constexpr int E = 8; using R = Radices<2, 8, 8>; };
+template <> struct Plan<256> { static constexpr int E = 8; using R = Radices<4, 8, 8>; };
+template <> struct Plan<512> { static constexpr int E = 8; using R = Radices<8, 8, 8>; };
+template <> struct Plan<1024> { static constexpr int E = 16; using R = Radices<2, 8, 8, 8>; };
+// non power-of-two lengths used by uneven ensembles (x half lengths 24, 40, 48)
+template <> struct Plan<24> { static constexpr int E = 24; using R = Radices<3, 8>; };
+template <> struct Plan<40> { static constexpr int E = 20; using R = Radices<5, 2, 4>; };
+template <> struct Plan<48> { static constexpr int E = 12; using R = Radices<3, 4, 4>; };
+template <> struct Plan<80> { static constexpr int E = 20; using R = Radices<5, 4, 4>; };
+template <> struct Plan<96> { static constexpr int E = 24; using R = Radices<3, 4, 8>; };
+
+// One Stockham stage (radix R, input sub-length Ns) and the stages after it.
+template <typename C, int N, int E, int DIR, int TWS, int Ns, int R, int... Rest>
+__device__ __forceinline__ void stages(C (&v)[E], C *sm, int ld, int c, int j, const C *tw) {
+  constexpr int T = N / E;
+  constexpr int B = E / R;
+  constexpr bool last = sizeof...(Rest) == 0;
+  static_assert(E % R == 0, "plan: radix must divide E");
+#pragma unroll
+  for (int t = 0; t < B; ++t) {
+    C x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = v[t + r * B];
+    const int b = j + t * T;
+    const int k = (Ns > 1) ? (b % Ns) : 0;
+    if (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) x[r] = twmul<DIR>(x[r], tw[k * r * (TWS / (Ns * R))]);
+    }
+    Dft<R, DIR, C>::run(x);
+    if (last) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[t + r * B] = x[r];
+    } else {
+      const int base = (b / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) sm[(base + r * Ns) * ld + c] = x[r];
+    }
+  }
+  if constexpr (!last) {
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = sm[(j + T * m) * ld + c];
+    __syncthreads();
+    stages<C, N, E, DIR, TWS, Ns * R, Rest...>(v, sm, ld, c, j, tw);
+  }
+}
+
+template <typename C, int N, int E, int DIR, int TWS, int... Rs>
+__device__ __forceinline__ void fft_run(Radices<Rs...>, C (&v)[E], C *sm, int ld, int c, int j,
+                                        const C *tw) {
+  if constexpr (sizeof...(Rs) > 0) stages<C, N, E, DIR, TWS, 1, Rs...>(v, sm, ld, c, j, tw);
+}
+
+// Transform one line of length N held as v[m] at positions j + (N/E)*m.
+template <typename C, int N, int DIR, int TWS>
+__device__ __forceinline__ void fft_line(C (&v)[Plan<N>::E], C *sm, int ld, int c, int j,
+                                         const C *tw) {
+  fft_run<C, N, Plan<N>::E, DIR, TWS>(typename Plan<N>::R{}, v, sm, ld, c, j, tw);
+}
+
+}  // namespace opfc

@@ -1,0 +1,709 @@
+// kernels.cuh -- the pass kernels of the spectral PFC step (sm_100a).
+//
+// One PFC step with the state psi_hat resident in k-space is four passes over
+// the spectrum (the reference runs 3-4 full 3D FFTs plus 3-4 elementwise sweeps,
+// apps/tungsten/include/tungsten/cuda/tungsten_model.hpp:392-455):
+//
+//   YI  inverse y transform of A = F_z^-1[psi_hat]                (col pass)
+//   X   per x-row: C2R -> nonlinearity -> R2C, in place on A       (x pass)
+//   YF  forward y transform                                        (col pass)
+//   ZU  forward z transform of N_hat, ETD update psi_hat = opL psi_hat + opN
+//       N_hat (in place), inverse z transform of the new state into A   (col pass)
+//
+// plus a tiny Hermitian projection of the kx = 0 and Nyquist planes.  Every
+// pass reads and writes each mode once; the nonlinearity, the mean-field filter
+// and the k-space update never make a sweep of their own.
+#pragma once
+#include "fft_core.cuh"
+#include "launch.h"
+
+namespace opfc {
+
+template <typename Real> struct Width;       // columns / rows per CTA
+template <> struct Width<float> { static constexpr int W = 16; };
+template <> struct Width<double> { static constexpr int W = 8; };
+
+template <typename Real> struct ColArgs {
+  ColSeg seg0, seg1;
+  const void *in[2];
+  void *out[2];
+  const void *tw;
+  void *psi_hat;
+  const Real *tab_a, *tab_b, *tab_chi;
+};
+
+template <typename C> __device__ __forceinline__ C czero() { return mk<C>(0, 0); }
+
+// ---------------------------------------------------------------------------
+// column pass: batched FFT along a strided axis (y or z), optional ETD update
+// ---------------------------------------------------------------------------
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
+__global__ void __launch_bounds__(Width<Real>::W *(N / Plan<N>::E))
+    col_kernel(const ColArgs<Real> a) {
+  using C = typename Cx<Real>::T;
+  constexpr int W = Width<Real>::W;
+  constexpr int E = Plan<N>::E;
+  constexpr int T = N / E;
+  constexpr int NT = W * T;
+  constexpr int ld = W + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *sm = tw + N;
+
+  const int tid = threadIdx.x;
+  const int c = tid % W;
+  const int j = tid / W;
+  const C *gtw = reinterpret_cast<const C *>(a.tw);
+  for (int i = tid; i < N; i += NT) tw[i] = gtw[i];
+
+  int t = blockIdx.x;
+  const bool second = t >= a.seg0.ntiles;
+  const ColSeg sg = second ? a.seg1 : a.seg0;
+  if (second) t -= a.seg0.ntiles;
+  const int ti = t % sg.tiles_inner;
+  const int to = t / sg.tiles_inner;
+  const int cg = ti * W + c;
+  const bool ok = cg < sg.ncols;
+  const long long base = sg.off + (long long)to * sg.s_outer + (long long)cg * sg.col_stride;
+  const long long fs = sg.fft_stride;
+  const int set = blockIdx.y;
+  const C *in = reinterpret_cast<const C *>(a.in[set]);
+  C *out = reinterpret_cast<C *>(a.out[set]);
+
+  C v[E];
+#pragma unroll
+  for (int m = 0; m < E; ++m) v[m] = ok ? in[base + (long long)(j + T * m) * fs] : czero<C>();
+
+  if constexpr (MODE == COL_PLAIN) {
+    fft_line<C, N, DIR, N>(v, sm, ld, c, j, tw);
+    if (ok) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) out[base + (long long)(j + T * m) * fs] = v[m];
+    }
+  } else {
+    // forward z transform completes N_hat; ETD update of the resident state
+    fft_line<C, N, -1, N>(v, sm, ld, c, j, tw);
+    C *ph = reinterpret_cast<C *>(a.psi_hat);
+    C w[(MODEL == MK_PLAIN) ? 1 : E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const long long idx = base + (long long)(j + T * m) * fs;
+      C np = czero<C>();
+      if (ok) {
+        const C p = ph[idx];
+        const Real la = a.tab_a[idx];
+        const Real lb = a.tab_b[idx];
+        np = mk<C>(la * p.x + lb * v[m].x, la * p.y + lb * v[m].y);
+        ph[idx] = np;
+        if constexpr (MODEL != MK_PLAIN) {
+          const Real ch = a.tab_chi[idx];
+          w[m] = cscale(np, ch);
+        }
+      } else if constexpr (MODEL != MK_PLAIN) {
+        w[m] = czero<C>();
+      }
+      v[m] = np;
+    }
+    if constexpr (INV) {
+      if constexpr (MODEL == MK_FILTERED) {
+        fft_line<C, N, +1, N>(w, sm, ld, c, j, tw);
+        if (ok) {
+#pragma unroll
+          for (int m = 0; m < E; ++m) out[base + (long long)(j + T * m) * fs] = w[m];
+        }
+      } else {
+        fft_line<C, N, +1, N>(v, sm, ld, c, j, tw);
+        if (ok) {
+#pragma unroll
+          for (int m = 0; m < E; ++m) out[base + (long long)(j + T * m) * fs] = v[m];
+        }
+        if constexpr (MODEL == MK_TUNGSTEN) {
+          C *out2 = reinterpret_cast<C *>(a.out[1]);
+          fft_line<C, N, +1, N>(w, sm, ld, c, j, tw);
+          if (ok) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) out2[base + (long long)(j + T * m) * fs] = w[m];
+          }
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// x pass: each row of N0 = 2M reals <-> M+1 complex modes, via one complex FFT
+// of length M of z[p] = x[2p] + i x[2p+1] and the split/merge post-processing.
+// ---------------------------------------------------------------------------
+template <typename Real> struct XArgs {
+  const void *in0, *in1;
+  void *out;
+  const Real *rin;
+  Real *rout;
+  const void *tw;
+  long long nyq_off;
+  int rows;
+  double scale, mean;
+  Real c0, c1, c2, c3, c4, c5;
+  unsigned int *flag;
+};
+
+// rows [row0, row0+W) of a split-layout complex array -> smem buf[k][c], k<=M
+template <typename C, int M, int W, int NT>
+__device__ __forceinline__ void x_load_rows(const C *in, long long nyq_off, int row0, int rows,
+                                            C *buf, int tid) {
+  constexpr int ld = W + 1;
+  for (int f = tid; f < W * M; f += NT) {
+    const int cc = f / M, k = f - cc * M;
+    const int row = row0 + cc;
+    buf[k * ld + cc] = (row < rows) ? in[(long long)row * M + k] : mk<C>(0, 0);
+  }
+  if (tid < W) {
+    const int row = row0 + tid;
+    buf[M * ld + tid] = (row < rows) ? in[nyq_off + row] : mk<C>(0, 0);
+  }
+}
+
+// C2R pre-processing: Z'[k] = (X[k] + conj X[M-k]) + i e^{+2 pi i k/N0} (X[k] - conj X[M-k]),
+// with the imaginary parts of the DC and Nyquist bins ignored (C2R semantics).
+template <typename C, int M, int W, int E>
+__device__ __forceinline__ void x_pre(const C *buf, const C *tw, int c, int j, C (&v)[E]) {
+  constexpr int ld = W + 1;
+  constexpr int T = M / E;
+#pragma unroll
+  for (int m = 0; m < E; ++m) {
+    const int k = j + T * m;
+    C X = buf[k * ld + c];
+    C Y = buf[(M - k) * ld + c];
+    if (k == 0) {
+      X.y = 0;
+      Y.y = 0;
+    }
+    const C s = mk<C>(X.x + Y.x, X.y - Y.y);
+    const C d = mk<C>(X.x - Y.x, X.y + Y.y);
+    const C e = twmul<+1>(d, tw[k]);  // d * e^{+2 pi i k / N0}
+    v[m] = mk<C>(s.x - e.y, s.y + e.x);
+  }
+}
+
+// R2C post-processing and store:
+// X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 e^{-2 pi i k/N0} (Z[k] - conj Z[M-k]),
+// X[M] = Re Z[0] - Im Z[0].
+template <typename C, int M, int W, int NT>
+__device__ __forceinline__ void x_post_store(const C *buf, const C *tw, C *out, long long nyq_off,
+                                             int row0, int rows, int tid) {
+  using S = decltype(C::x);
+  constexpr int ld = W + 1;
+  for (int f = tid; f < W * M; f += NT) {
+    const int cc = f / M, k = f - cc * M;
+    const int row = row0 + cc;
+    const int km = (k == 0) ? 0 : M - k;
+    const C Z = buf[k * ld + cc];
+    const C Y = buf[km * ld + cc];
+    const C s = mk<C>(Z.x + Y.x, Z.y - Y.y);
+    const C d = mk<C>(Z.x - Y.x, Z.y + Y.y);
+    const C e = twmul<-1>(d, tw[k]);  // d * e^{-2 pi i k / N0}
+    const C X = mk<C>(S(0.5) * (s.x + e.y), S(0.5) * (s.y - e.x));
+    if (row < rows) out[(long long)row * M + k] = X;
+  }
+  if (tid < W) {
+    const int row = row0 + tid;
+    const C Z = buf[tid];
+    if (row < rows) out[nyq_off + row] = mk<C>(Z.x - Z.y, S(0));
+  }
+}
+
+template <typename Real>
+__device__ __forceinline__ Real to_real_plus_mean(Real z, double scale, double mean) {
+  return (Real)((double)z * scale + mean);
+}
+
+template <typename Real, int M, int MODE, int MODEL>
+__global__ void __launch_bounds__(Width<Real>::W *(M / Plan<M>::E)) x_kernel(const XArgs<Real> a) {
+  using C = typename Cx<Real>::T;
+  constexpr int W = Width<Real>::W;
+  constexpr int E = Plan<M>::E;
+  constexpr int T = M / E;
+  constexpr int NT = W * T;
+  constexpr int ld = W + 1;
+  constexpr int N0 = 2 * M;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *buf = tw + N0;
+
+  const int tid = threadIdx.x;
+  const int c = tid % W;
+  const int j = tid / W;
+  const C *gtw = reinterpret_cast<const C *>(a.tw);
+  for (int i = tid; i < N0; i += NT) tw[i] = gtw[i];
+  const int row0 = blockIdx.x * W;
+  C v[E];
+
+  if constexpr (MODE == X_R2C) {
+    // real rows -> buf[p][c] as (x[2p], x[2p+1])
+    for (int f = tid; f < W * M; f += NT) {
+      const int cc = f / M, p = f - cc * M;
+      const int row = row0 + cc;
+      C z = mk<C>(0, 0);
+      if (row < a.rows) z = reinterpret_cast<const C *>(a.rin + (long long)row * N0)[p];
+      buf[p * ld + cc] = z;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = buf[(j + T * m) * ld + c];
+    __syncthreads();
+    fft_line<C, M, -1, N0>(v, buf, ld, c, j, tw);
+  } else {
+    const C *in0 = reinterpret_cast<const C *>(a.in0);
+    x_load_rows<C, M, W, NT>(in0, a.nyq_off, row0, a.rows, buf, tid);
+    __syncthreads();
+    x_pre<C, M, W, E>(buf, tw, c, j, v);
+    __syncthreads();
+    fft_line<C, M, +1, N0>(v, buf, ld, c, j, tw);
+#pragma unroll
+    for (int m = 0; m < E; ++m)
+      v[m] = mk<C>(to_real_plus_mean(v[m].x, a.scale, a.mean),
+                   to_real_plus_mean(v[m].y, a.scale, a.mean));
+    if constexpr (MODE == X_C2R) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) buf[(j + T * m) * ld + c] = v[m];
+      __syncthreads();
+      for (int f = tid; f < W * M; f += NT) {
+        const int cc = f / M, p = f - cc * M;
+        const int row = row0 + cc;
+        if (row < a.rows) reinterpret_cast<C *>(a.rout + (long long)row * N0)[p] = buf[p * ld + cc];
+      }
+      return;
+    } else {
+      bool bad = false;
+      if constexpr (MODEL == MK_TUNGSTEN) {
+        C u[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) u[m] = v[m];
+        const C *in1 = reinterpret_cast<const C *>(a.in1);
+        // buf is free: the inverse FFT's last stage only touched registers
+        x_load_rows<C, M, W, NT>(in1, a.nyq_off, row0, a.rows, buf, tid);
+        __syncthreads();
+        x_pre<C, M, W, E>(buf, tw, c, j, v);
+        __syncthreads();
+        fft_line<C, M, +1, N0>(v, buf, ld, c, j, tw);
+        // N = p3b u^2 + p4b u^3 + q3b v^2 + q4b v^3 - stabP u
+        // (apps/tungsten/include/tungsten/cpu/tungsten_model.hpp:334-350)
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          const Real vx = to_real_plus_mean(v[m].x, a.scale, a.mean);
+          const Real vy = to_real_plus_mean(v[m].y, a.scale, a.mean);
+          const Real ux = u[m].x, uy = u[m].y;
+          const Real nx = a.c0 * ux * ux + a.c1 * ux * ux * ux + a.c2 * vx * vx +
+                          a.c3 * vx * vx * vx - a.c4 * ux;
+          const Real ny = a.c0 * uy * uy + a.c1 * uy * uy * uy + a.c2 * vy * vy +
+                          a.c3 * vy * vy * vy - a.c4 * uy;
+          bad |= !(isfinite(nx) && isfinite(ny));
+          v[m] = mk<C>(nx, ny);
+        }
+      } else if constexpr (MODEL == MK_FILTERED) {
+        // N = p2 v^2/2 + p3 v^3/3 + p4 v^4/4 of the filtered density
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          const Real x = v[m].x, y = v[m].y;
+          const Real x2 = x * x, y2 = y * y;
+          const Real nx = x2 * (a.c0 + a.c1 * x + a.c2 * x2);
+          const Real ny = y2 * (a.c0 + a.c1 * y + a.c2 * y2);
+          bad |= !(isfinite(nx) && isfinite(ny));
+          v[m] = mk<C>(nx, ny);
+        }
+      } else {
+        // N = psi^3 (docs/api/examples/10_complete_pfc_model.cpp:128-130)
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          const Real x = v[m].x, y = v[m].y;
+          const Real nx = x * x * x, ny = y * y * y;
+          bad |= !(isfinite(nx) && isfinite(ny));
+          v[m] = mk<C>(nx, ny);
+        }
+      }
+      if (bad && a.flag) atomicOr(a.flag, 1u);
+      fft_line<C, M, -1, N0>(v, buf, ld, c, j, tw);
+    }
+  }
+  // Z in registers -> buf -> post-process -> store
+#pragma unroll
+  for (int m = 0; m < E; ++m) buf[(j + T * m) * ld + c] = v[m];
+  __syncthreads();
+  x_post_store<C, M, W, NT>(buf, tw, reinterpret_cast<C *>(a.out), a.nyq_off, row0, a.rows, tid);
+}
+
+// ---------------------------------------------------------------------------
+// small helper kernels (not on the per-step hot path except herm_fix)
+// ---------------------------------------------------------------------------
+
+// Hermitian projection of the kx = 0 and kx = N0/2 planes: a real field's
+// spectrum satisfies X(0,-ky,-kz) = conj X(0,ky,kz) there; the C2R ignores the
+// anti-Hermitian part, so it is removed from the resident state instead of
+// being left to grow under exp(L dt) > 1.
+template <typename Real>
+__global__ void herm_fix_kernel(typename Cx<Real>::T *psi, long long nyq_off, int M, int n1, int n2) {
+  using C = typename Cx<Real>::T;
+  const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long plane = (long long)n1 * n2;
+  if (e >= plane) return;
+  const int y = (int)(e % n1), z = (int)(e / n1);
+  const int yp = (n1 - y) % n1, zp = (n2 - z) % n2;
+  const long long p = (long long)yp + (long long)n1 * zp;
+  C *P;
+  long long stride;
+  if (blockIdx.y == 0) {
+    P = psi;
+    stride = M;
+  } else {
+    P = psi + nyq_off;
+    stride = 1;
+  }
+  if (e < p) {
+    const C u = P[e * stride], w = P[p * stride];
+    const C h = mk<C>(Real(0.5) * (u.x + w.x), Real(0.5) * (u.y - w.y));
+    P[e * stride] = h;
+    P[p * stride] = mk<C>(h.x, -h.y);
+  } else if (e == p) {
+    P[e * stride].y = 0;
+  }
+}
+
+template <typename Real, typename Out>
+__global__ void to_ref_kernel(const typename Cx<Real>::T *in, Out *out, int M, int n1, int n2,
+                              long long nyq_off, int dc_override, double dc_re) {
+  const long long nc = (long long)(M + 1) * n1 * n2;
+  for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < nc;
+       o += (long long)gridDim.x * blockDim.x) {
+    const long long row = o / (M + 1);
+    const int kx = (int)(o - row * (M + 1));
+    typename Cx<Real>::T v = (kx < M) ? in[row * M + kx] : in[nyq_off + row];
+    double re = v.x, im = v.y;
+    if (dc_override && o == 0) {
+      re = dc_re;
+      im = 0;
+    }
+    out[2 * o] = (Out)re;
+    out[2 * o + 1] = (Out)im;
+  }
+}
+
+template <typename Real, typename In>
+__global__ void from_ref_kernel(const In *in, typename Cx<Real>::T *out, int M, int n1, int n2,
+                                long long nyq_off) {
+  const long long nc = (long long)(M + 1) * n1 * n2;
+  for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < nc;
+       o += (long long)gridDim.x * blockDim.x) {
+    const long long row = o / (M + 1);
+    const int kx = (int)(o - row * (M + 1));
+    typename Cx<Real>::T v;
+    v.x = (Real)in[2 * o];
+    v.y = (Real)in[2 * o + 1];
+    if (kx < M)
+      out[row * M + kx] = v;
+    else
+      out[nyq_off + row] = v;
+  }
+}
+
+template <typename In, typename Out>
+__global__ void cast_kernel(const In *in, Out *out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (Out)in[i];
+}
+
+// FP64 partial sums with Neumaier compensation per thread and per block.
+template <typename Real>
+__global__ void sum_pow_kernel(const Real *x, size_t n, int p, double *partials) {
+  __shared__ double rs[256], rc[256];
+  double s = 0, c = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const double v0 = x[i];
+    const double v = (p == 4) ? (v0 * v0) * (v0 * v0) : v0;
+    const double t = s + v;
+    c += (fabs(s) >= fabs(v)) ? (s - t) + v : (v - t) + s;
+    s = t;
+  }
+  rs[threadIdx.x] = s;
+  rc[threadIdx.x] = c;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) {
+      const double a = rs[threadIdx.x], b = rs[threadIdx.x + h];
+      const double t = a + b;
+      rc[threadIdx.x] += rc[threadIdx.x + h] + ((fabs(a) >= fabs(b)) ? (a - t) + b : (b - t) + a);
+      rs[threadIdx.x] = t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = rs[0] + rc[0];
+}
+
+struct EnergyK {
+  double f0, f1, f2, r;
+};
+
+__device__ __forceinline__ double kcomp(int i, int n, double f) {
+  return (i <= n / 2) ? i * f : (i - n) * f;
+}
+
+template <typename Real>
+__global__ void energy_k_kernel(const typename Cx<Real>::T *ph, int M, int n1, int n2,
+                                long long nyq_off, EnergyK ek, double *partials) {
+  __shared__ double red[256];
+  const long long nc = (long long)(M + 1) * n1 * n2;
+  const int n0 = 2 * M;
+  double s = 0;
+  for (long long o = (long long)blockIdx.x * blockDim.x + threadIdx.x; o < nc;
+       o += (long long)gridDim.x * blockDim.x) {
+    int kx, ky, kz;
+    typename Cx<Real>::T v;
+    if (o < (long long)M * n1 * n2) {
+      kx = (int)(o % M);
+      const long long row = o / M;
+      ky = (int)(row % n1);
+      kz = (int)(row / n1);
+      v = ph[o];
+    } else {
+      const long long row = o - (long long)M * n1 * n2;
+      kx = M;
+      ky = (int)(row % n1);
+      kz = (int)(row / n1);
+      v = ph[nyq_off + row];
+    }
+    const double kxx = kcomp(kx, n0, ek.f0), kyy = kcomp(ky, n1, ek.f1), kzz = kcomp(kz, n2, ek.f2);
+    const double k2 = kxx * kxx + kyy * kyy + kzz * kzz;
+    const double G = ek.r + (1.0 - k2) * (1.0 - k2);
+    const double wgt = (kx == 0 || kx == M) ? 1.0 : 2.0;
+    s += wgt * G * ((double)v.x * v.x + (double)v.y * v.y);
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+    if (threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
+static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
+  using C = typename Cx<Real>::T;
+  constexpr int W = Width<Real>::W;
+  constexpr int NT = W * (N / Plan<N>::E);
+  const size_t smem = sizeof(C) * ((size_t)N + (size_t)N * (W + 1));
+  auto k = col_kernel<Real, N, MODE, DIR, MODEL, INV>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  ColArgs<Real> a;
+  a.seg0 = L.seg[0];
+  a.seg1 = L.seg[1];
+  if (L.nseg < 2) a.seg1.ntiles = 0;
+  a.in[0] = L.in[0];
+  a.in[1] = L.in[1];
+  a.out[0] = L.out[0];
+  a.out[1] = L.out[1];
+  a.tw = L.tw;
+  a.psi_hat = L.psi_hat;
+  a.tab_a = reinterpret_cast<const Real *>(L.tab_a);
+  a.tab_b = reinterpret_cast<const Real *>(L.tab_b);
+  a.tab_chi = reinterpret_cast<const Real *>(L.tab_chi);
+  const int tiles = a.seg0.ntiles + a.seg1.ntiles;
+  if (tiles == 0) return 0;
+  dim3 grid(tiles, MODE == COL_PLAIN ? L.nsets : 1);
+  k<<<grid, NT, smem, s>>>(a);
+  return (int)cudaGetLastError();
+}
+
+template <typename Real, int N>
+static int launch_col_n(const ColLaunch &L, cudaStream_t s) {
+  if (L.mode == COL_PLAIN) {
+    if (L.dir < 0) return launch_col_t<Real, N, COL_PLAIN, -1, 0, false>(L, s);
+    return launch_col_t<Real, N, COL_PLAIN, +1, 0, false>(L, s);
+  }
+  switch (L.model) {
+    case MK_PLAIN:
+      return L.inverse_after ? launch_col_t<Real, N, COL_UPDATE, -1, MK_PLAIN, true>(L, s)
+                             : launch_col_t<Real, N, COL_UPDATE, -1, MK_PLAIN, false>(L, s);
+    case MK_TUNGSTEN:
+      return L.inverse_after ? launch_col_t<Real, N, COL_UPDATE, -1, MK_TUNGSTEN, true>(L, s)
+                             : launch_col_t<Real, N, COL_UPDATE, -1, MK_TUNGSTEN, false>(L, s);
+    case MK_FILTERED:
+      return L.inverse_after ? launch_col_t<Real, N, COL_UPDATE, -1, MK_FILTERED, true>(L, s)
+                             : launch_col_t<Real, N, COL_UPDATE, -1, MK_FILTERED, false>(L, s);
+  }
+  return (int)cudaErrorInvalidValue;
+}
+
+template <typename Real, int M, int MODE, int MODEL>
+static int launch_x_t(const XLaunch &L, cudaStream_t s) {
+  using C = typename Cx<Real>::T;
+  constexpr int W = Width<Real>::W;
+  constexpr int NT = W * (M / Plan<M>::E);
+  const size_t smem = sizeof(C) * ((size_t)2 * M + (size_t)(M + 1) * (W + 1));
+  auto k = x_kernel<Real, M, MODE, MODEL>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  XArgs<Real> a;
+  a.in0 = L.in0;
+  a.in1 = L.in1;
+  a.out = L.out;
+  a.rin = reinterpret_cast<const Real *>(L.rin);
+  a.rout = reinterpret_cast<Real *>(L.rout);
+  a.tw = L.tw;
+  a.nyq_off = L.nyq_off;
+  a.rows = L.rows;
+  a.scale = L.scale;
+  a.mean = L.mean;
+  a.c0 = (Real)L.c[0];
+  a.c1 = (Real)L.c[1];
+  a.c2 = (Real)L.c[2];
+  a.c3 = (Real)L.c[3];
+  a.c4 = (Real)L.c[4];
+  a.c5 = (Real)L.c[5];
+  a.flag = L.flag;
+  const int blocks = (L.rows + W - 1) / W;
+  k<<<blocks, NT, smem, s>>>(a);
+  return (int)cudaGetLastError();
+}
+
+template <typename Real, int M>
+static int launch_x_m(const XLaunch &L, cudaStream_t s) {
+  if (L.mode == X_R2C) return launch_x_t<Real, M, X_R2C, 0>(L, s);
+  if (L.mode == X_C2R) return launch_x_t<Real, M, X_C2R, 0>(L, s);
+  switch (L.model) {
+    case MK_PLAIN: return launch_x_t<Real, M, X_FUSED, MK_PLAIN>(L, s);
+    case MK_TUNGSTEN: return launch_x_t<Real, M, X_FUSED, MK_TUNGSTEN>(L, s);
+    case MK_FILTERED: return launch_x_t<Real, M, X_FUSED, MK_FILTERED>(L, s);
+  }
+  return (int)cudaErrorInvalidValue;
+}
+
+#define OPFC_SIZES(X) X(2) X(4) X(8) X(16) X(24) X(32) X(40) X(48) X(64) X(80) X(96) X(128) X(256) X(512) X(1024)
+
+template <typename Real> int launch_col(const ColLaunch &L, cudaStream_t s) {
+  switch (L.N) {
+#define OPFC_CASE(n) \
+  case n: return launch_col_n<Real, n>(L, s);
+    OPFC_SIZES(OPFC_CASE)
+#undef OPFC_CASE
+    case 1:
+      if (L.mode == COL_PLAIN && L.in[0] == L.out[0] && (L.nsets < 2 || L.in[1] == L.out[1])) return 0;
+      return launch_col_n<Real, 1>(L, s);
+  }
+  return (int)cudaErrorInvalidValue;
+}
+
+template <typename Real> int launch_x(const XLaunch &L, cudaStream_t s) {
+  switch (L.M) {
+#define OPFC_CASE(n) \
+  case n: return launch_x_m<Real, n>(L, s);
+    OPFC_SIZES(OPFC_CASE)
+#undef OPFC_CASE
+    case 1: return launch_x_m<Real, 1>(L, s);
+  }
+  return (int)cudaErrorInvalidValue;
+}
+
+template <typename Real>
+int launch_herm_fix(void *psi, long long nyq_off, int M, int n1, int n2, cudaStream_t s) {
+  const long long plane = (long long)n1 * n2;
+  dim3 grid((unsigned)((plane + 255) / 256), 2);
+  herm_fix_kernel<Real><<<grid, 256, 0, s>>>(reinterpret_cast<typename Cx<Real>::T *>(psi), nyq_off,
+                                             M, n1, n2);
+  return (int)cudaGetLastError();
+}
+
+static inline int grid_for(long long n) {
+  long long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  if (b < 1) b = 1;
+  return (int)b;
+}
+
+template <typename Real>
+int launch_to_ref(const void *in, void *out, int out_is_f64, int M, int n1, int n2, long long nyq_off,
+                  int dc_override, double dc_re, cudaStream_t s) {
+  const long long nc = (long long)(M + 1) * n1 * n2;
+  const auto *pin = reinterpret_cast<const typename Cx<Real>::T *>(in);
+  if (out_is_f64)
+    to_ref_kernel<Real, double><<<grid_for(nc), 256, 0, s>>>(pin, (double *)out, M, n1, n2, nyq_off,
+                                                             dc_override, dc_re);
+  else
+    to_ref_kernel<Real, float><<<grid_for(nc), 256, 0, s>>>(pin, (float *)out, M, n1, n2, nyq_off,
+                                                            dc_override, dc_re);
+  return (int)cudaGetLastError();
+}
+
+template <typename Real>
+int launch_from_ref(const void *in, int in_is_f64, void *out, int M, int n1, int n2, long long nyq_off,
+                    cudaStream_t s) {
+  const long long nc = (long long)(M + 1) * n1 * n2;
+  auto *pout = reinterpret_cast<typename Cx<Real>::T *>(out);
+  if (in_is_f64)
+    from_ref_kernel<Real, double><<<grid_for(nc), 256, 0, s>>>((const double *)in, pout, M, n1, n2,
+                                                               nyq_off);
+  else
+    from_ref_kernel<Real, float><<<grid_for(nc), 256, 0, s>>>((const float *)in, pout, M, n1, n2,
+                                                              nyq_off);
+  return (int)cudaGetLastError();
+}
+
+template <typename Real>
+int launch_cast_real(const void *in, int in_is_f64, void *out, int out_is_f64, size_t n,
+                     cudaStream_t s) {
+  const int g = grid_for((long long)n);
+  if (in_is_f64 && out_is_f64)
+    cast_kernel<double, double><<<g, 256, 0, s>>>((const double *)in, (double *)out, n);
+  else if (in_is_f64)
+    cast_kernel<double, float><<<g, 256, 0, s>>>((const double *)in, (float *)out, n);
+  else if (out_is_f64)
+    cast_kernel<float, double><<<g, 256, 0, s>>>((const float *)in, (double *)out, n);
+  else
+    cast_kernel<float, float><<<g, 256, 0, s>>>((const float *)in, (float *)out, n);
+  return (int)cudaGetLastError();
+}
+
+template <typename Real>
+int launch_sum_pow(const void *x, size_t n, int p, double *partials, int nblocks, cudaStream_t s) {
+  sum_pow_kernel<Real><<<nblocks, 256, 0, s>>>(reinterpret_cast<const Real *>(x), n, p, partials);
+  return (int)cudaGetLastError();
+}
+
+template <typename Real>
+int launch_energy_k(const void *psi_hat, int M, int n1, int n2, long long nyq_off, const double *dx,
+                    double r, double *partials, int nblocks, cudaStream_t s) {
+  const double two_pi = 6.283185307179586476925286766559;
+  EnergyK ek;
+  ek.f0 = two_pi / (dx[0] * (2 * M));
+  ek.f1 = two_pi / (dx[1] * n1);
+  ek.f2 = two_pi / (dx[2] * n2);
+  ek.r = r;
+  energy_k_kernel<Real><<<nblocks, 256, 0, s>>>(
+      reinterpret_cast<const typename Cx<Real>::T *>(psi_hat), M, n1, n2, nyq_off, ek, partials);
+  return (int)cudaGetLastError();
+}
+
+#define OPFC_INSTANTIATE(R)                                                                          \
+  template int launch_col<R>(const ColLaunch &, cudaStream_t);                                       \
+  template int launch_x<R>(const XLaunch &, cudaStream_t);                                           \
+  template int launch_herm_fix<R>(void *, long long, int, int, int, cudaStream_t);                   \
+  template int launch_to_ref<R>(const void *, void *, int, int, int, int, long long, int, double,    \
+                                cudaStream_t);                                                       \
+  template int launch_from_ref<R>(const void *, int, void *, int, int, int, long long, cudaStream_t); \
+  template int launch_cast_real<R>(const void *, int, void *, int, size_t, cudaStream_t);            \
+  template int launch_sum_pow<R>(const void *, size_t, int, double *, int, cudaStream_t);            \
+  template int launch_energy_k<R>(const void *, int, int, int, long long, const double *, double,    \
+                                  double *, int, cudaStream_t);
+
+}  // namespace opfc

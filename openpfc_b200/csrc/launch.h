@@ -1,0 +1,96 @@
+// launch.h -- host-side launch descriptors shared by the C-ABI and the kernels.
+//
+// Internal k-space layout ("split half spectrum"): for a grid N0 x N1 x N2 with
+// M = N0/2, the Nc = (M+1) N1 N2 modes are stored as
+//   main[kx + M (ky + N1 kz)]     for kx in [0, M)      (M*N1*N2 elements)
+//   nyq [ky + N1 kz]              for kx = M (Nyquist)  (N1*N2 elements)
+// in one allocation (nyq right after main).  Every main row is M complex values,
+// so tiles of W consecutive kx are aligned, full-width HBM segments; the
+// reference layout ((M+1) values per row, fft.cpp:58-70) is produced only at
+// the ABI boundary.
+#pragma once
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace opfc {
+
+// One family of column tiles.  Tile t covers columns [ti*W, ti*W + W) of the
+// outer index `to`, with ti = t % tiles_inner and to = t / tiles_inner.
+struct ColSeg {
+  long long off;         // element offset of outer index 0, column 0
+  long long s_outer;     // element stride between outer indices
+  long long fft_stride;  // element stride along the transformed axis
+  long long col_stride;  // element stride between neighbouring columns
+  int tiles_inner;       // tiles per outer index
+  int ncols;             // columns per outer index (bounds check)
+  int ntiles;            // tiles in this family
+  int pad_;
+};
+
+enum ColMode { COL_PLAIN = 0, COL_UPDATE = 1 };
+enum ModelKind { MK_PLAIN = 0, MK_TUNGSTEN = 1, MK_FILTERED = 2 };
+
+struct ColLaunch {
+  int N;        // transform length
+  int dir;      // -1 forward, +1 inverse (COL_PLAIN)
+  int mode;     // ColMode
+  int model;    // ModelKind (COL_UPDATE)
+  int nsets;    // 1 or 2 independent arrays (blockIdx.y)
+  int inverse_after;  // COL_UPDATE: also write the inverse transform(s)
+  ColSeg seg[2];
+  int nseg;
+  const void *in[2];
+  void *out[2];
+  const void *tw;     // exp(-2 pi i k / N), N entries, compute precision
+  // COL_UPDATE operands (all in the split layout, compute precision)
+  void *psi_hat;      // state, updated in place
+  const void *tab_a;  // opL / exp_Ldt
+  const void *tab_b;  // opN / n_weight
+  const void *tab_chi;  // mean-field filter (TUNGSTEN, FILTERED)
+};
+
+enum XMode { X_R2C = 0, X_C2R = 1, X_FUSED = 2 };
+
+struct XLaunch {
+  int M;           // N0 / 2 (half length of the real transform)
+  int rows;        // N1 * N2
+  int mode;        // XMode
+  int model;       // ModelKind (X_FUSED)
+  long long nyq_off;
+  const void *in0;   // complex input (split layout)
+  const void *in1;   // second complex input (TUNGSTEN psi_MF)
+  void *out;         // complex output (split layout)
+  const void *rin;   // real rows (X_R2C)
+  void *rout;        // real rows (X_C2R)
+  const void *tw;    // exp(-2 pi i k / N0), N0 = 2M entries
+  double scale;      // C2R normalisation 1/(N0 N1 N2)
+  double mean;       // mean density added after the C2R (k = 0 mode in FP64)
+  double c[8];       // nonlinearity coefficients
+  unsigned int *flag;  // set to 1 when a non-finite value is produced
+};
+
+// Kernel launchers (kernels_f32.cu / kernels_f64.cu).  Return cudaError_t as int.
+template <typename Real> int launch_col(const ColLaunch &a, cudaStream_t s);
+template <typename Real> int launch_x(const XLaunch &a, cudaStream_t s);
+template <typename Real>
+int launch_herm_fix(void *psi, long long nyq_off, int M, int n1, int n2, cudaStream_t s);
+template <typename Real>
+int launch_to_ref(const void *in, void *out, int out_is_f64, int M, int n1, int n2,
+                  long long nyq_off, int dc_override, double dc_re, cudaStream_t s);
+template <typename Real>
+int launch_from_ref(const void *in, int in_is_f64, void *out, int M, int n1, int n2,
+                    long long nyq_off, cudaStream_t s);
+template <typename Real>
+int launch_cast_real(const void *in, int in_is_f64, void *out, int out_is_f64, size_t n,
+                     cudaStream_t s);
+// FP64 partial sums of x (p = 1) or x^4 (p = 4); `partials` holds `nblocks`
+// doubles; the host finishes with a compensated sum.
+template <typename Real>
+int launch_sum_pow(const void *x, size_t n, int p, double *partials, int nblocks, cudaStream_t s);
+// FP64 partial sums of w_kx G(k) |psi_hat|^2 with G = r + (1 - k^2)^2.
+template <typename Real>
+int launch_energy_k(const void *psi_hat, int M, int n1, int n2, long long nyq_off,
+                    const double *dx, double r, double *partials, int nblocks, cudaStream_t s);
+
+}  // namespace opfc

@@ -1,0 +1,1067 @@
+// opfc.cu -- the C ABI (include/openpfc_b200.h): handle life cycle, FP64
+// operator tables, field I/O, the step sequence and its CUDA graph.
+//
+// Step sequence with the state psi_hat resident in k-space (split layout, see
+// launch.h) and one work array A that holds F_z^-1[psi_hat] between steps:
+//   YI(A) ; X(A: C2R -> N(psi) -> R2C) ; YF(A) ; ZU(A -> psi_hat, A) ; HERM(psi_hat)
+// The reference performs the same mathematics as
+// F[psi] -> multiply -> F^-1 -> nonlinearity -> F -> ETD combine -> F^-1
+// (apps/tungsten/include/tungsten/cpu/tungsten_model.hpp:306-366,
+//  docs/api/examples/10_complete_pfc_model.cpp:121-144).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/openpfc_b200.h"
+#include "launch.h"
+
+using namespace opfc;
+
+int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *out);
+
+namespace {
+
+constexpr double kPi = 3.14159265358979323846264338327950288;
+
+bool supported_len(int n) {
+  static const int ok[] = {1, 2, 4, 8, 16, 24, 32, 40, 48, 64, 80, 96, 128, 256, 512, 1024};
+  for (int v : ok)
+    if (v == n) return true;
+  return false;
+}
+
+// cos/sin(2 pi k / n) with octant reduction so that quarter turns are exact.
+void unit_root(long k, long n, double *c, double *s) {
+  k %= n;
+  if (k < 0) k += n;
+  if (n % 8 == 0) {
+    const long oct = (8 * k) / n;
+    const long rem = k - oct * (n / 8);
+    const double a = 2.0 * kPi * (double)rem / (double)n;
+    const double ca = std::cos(a), sa = std::sin(a);
+    const double r2 = 0.70710678118654752440084436210484903928;
+    double cc, ss;
+    switch (oct) {
+      case 0: cc = ca; ss = sa; break;
+      case 1: cc = r2 * (ca - sa); ss = r2 * (ca + sa); break;
+      case 2: cc = -sa; ss = ca; break;
+      case 3: cc = -r2 * (ca + sa); ss = r2 * (ca - sa); break;
+      case 4: cc = -ca; ss = -sa; break;
+      case 5: cc = -r2 * (ca - sa); ss = -r2 * (ca + sa); break;
+      case 6: cc = sa; ss = -ca; break;
+      default: cc = r2 * (ca + sa); ss = -r2 * (ca - sa); break;
+    }
+    *c = cc;
+    *s = ss;
+    return;
+  }
+  if (4 * k == n) { *c = 0; *s = 1; return; }
+  if (2 * k == n) { *c = -1; *s = 0; return; }
+  if (4 * k == 3 * n) { *c = 0; *s = -1; return; }
+  const double a = 2.0 * kPi * (double)k / (double)n;
+  *c = std::cos(a);
+  *s = std::sin(a);
+}
+
+double neumaier(const double *a, size_t n) {
+  double s = 0, c = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const double t = s + a[i];
+    if (std::fabs(s) >= std::fabs(a[i]))
+      c += (s - t) + a[i];
+    else
+      c += (a[i] - t) + s;
+    s = t;
+  }
+  return s + c;
+}
+
+template <typename F> void parallel_for(long n, F &&f) {
+  unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  if (n < 4096) nt = 1;
+  std::vector<std::thread> th;
+  const long chunk = (n + nt - 1) / nt;
+  for (unsigned t = 0; t < nt; ++t) {
+    const long lo = t * chunk, hi = std::min(n, lo + chunk);
+    if (lo >= hi) break;
+    th.emplace_back([lo, hi, &f] {
+      for (long i = lo; i < hi; ++i) f(i);
+    });
+  }
+  for (auto &x : th) x.join();
+}
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace
+
+struct opfc_handle {
+  opfc_desc desc{};
+  int n0 = 0, n1 = 0, n2 = 0, M = 0;
+  size_t nr = 0, nc = 0;
+  long long nyq_off = 0;
+  int prec = OPFC_FP32;
+  size_t rsz = 4;  // bytes per real in compute precision
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int device = 0;
+
+  void *psi_hat = nullptr;   // state (split layout, DC slot kept at zero)
+  void *work_a = nullptr;    // F_z^-1 of the state, then the step's working array
+  void *work_b = nullptr;    // TUNGSTEN: F_z^-1 of chi * state
+  void *tab_a = nullptr, *tab_b = nullptr, *tab_chi = nullptr;
+  void *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;
+  void *real_buf = nullptr;  // real-space staging (N0 N1 N2 reals)
+  unsigned int *flag = nullptr;
+  double *partials = nullptr;
+  int npartials = 1184;
+  size_t allocated = 0;
+
+  double mass_sum = 0.0;  // sum over cells of psi (the k = 0 mode), FP64
+  bool initialized = false;
+  bool have_state = false;
+  bool a_valid = false;
+  double dt = 0.0;
+
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t graph_exec = nullptr;
+  std::string err;
+};
+
+namespace {
+
+int fail(opfc_handle *h, int code, const char *fmt, ...) {
+  if (h) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    h->err = buf;
+  }
+  return code;
+}
+
+#define CUDA_TRY(h, expr)                                                                 \
+  do {                                                                                    \
+    cudaError_t e_ = (expr);                                                              \
+    if (e_ != cudaSuccess) return fail(h, OPFC_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString(e_)); \
+  } while (0)
+
+#define LAUNCH_TRY(h, expr)                                                                \
+  do {                                                                                     \
+    int e_ = (expr);                                                                       \
+    if (e_ != 0)                                                                           \
+      return fail(h, OPFC_ERR_CUDA, "%s: %s", #expr, cudaGetErrorString((cudaError_t)e_)); \
+  } while (0)
+
+int dev_alloc(opfc_handle *h, void **p, size_t bytes) {
+  cudaError_t e = cudaMalloc(p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(h, OPFC_ERR_OOM, "cudaMalloc(%zu bytes): %s", bytes, cudaGetErrorString(e));
+  }
+  h->allocated += bytes;
+  return OPFC_OK;
+}
+
+int upload_twiddles(opfc_handle *h, int n, void **dst) {
+  std::vector<double> d(2 * (size_t)n);
+  for (int k = 0; k < n; ++k) {
+    double c, s;
+    unit_root(k, n, &c, &s);
+    d[2 * k] = c;
+    d[2 * k + 1] = -s;
+  }
+  int rc = dev_alloc(h, dst, (size_t)n * 2 * h->rsz);
+  if (rc) return rc;
+  if (h->prec == OPFC_FP64) {
+    CUDA_TRY(h, cudaMemcpy(*dst, d.data(), d.size() * sizeof(double), cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float> f(d.begin(), d.end());
+    CUDA_TRY(h, cudaMemcpy(*dst, f.data(), f.size() * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  return OPFC_OK;
+}
+
+// split-layout index of reference mode (kx, ky, kz)
+inline size_t split_index(const opfc_handle *h, int kx, int ky, int kz) {
+  const size_t row = (size_t)ky + (size_t)h->n1 * (size_t)kz;
+  return kx < h->M ? (size_t)kx + (size_t)h->M * row : (size_t)h->nyq_off + row;
+}
+
+// Column-pass segments along y (axis 1) or z (axis 2), see launch.h.
+void col_segments(const opfc_handle *h, int axis, ColLaunch &L) {
+  const int W = (h->prec == OPFC_FP64) ? 8 : 16;
+  const int M = h->M, n1 = h->n1, n2 = h->n2;
+  ColSeg &a = L.seg[0];
+  ColSeg &b = L.seg[1];
+  a = ColSeg{};
+  b = ColSeg{};
+  a.col_stride = 1;
+  a.ncols = M;
+  a.tiles_inner = (M + W - 1) / W;
+  if (axis == 1) {
+    a.off = 0;
+    a.s_outer = (long long)M * n1;
+    a.fft_stride = M;
+    a.ntiles = a.tiles_inner * n2;
+    // Nyquist plane: y lines are contiguous, columns are the z index
+    b.off = h->nyq_off;
+    b.s_outer = 0;
+    b.fft_stride = 1;
+    b.col_stride = n1;
+    b.ncols = n2;
+    b.tiles_inner = (n2 + W - 1) / W;
+    b.ntiles = b.tiles_inner;
+  } else {
+    a.off = 0;
+    a.s_outer = M;
+    a.fft_stride = (long long)M * n1;
+    a.ntiles = a.tiles_inner * n1;
+    b.off = h->nyq_off;
+    b.s_outer = 0;
+    b.fft_stride = n1;
+    b.col_stride = 1;
+    b.ncols = n1;
+    b.tiles_inner = (n1 + W - 1) / W;
+    b.ntiles = b.tiles_inner;
+  }
+  L.nseg = 2;
+  L.N = (axis == 1) ? n1 : n2;
+}
+
+int col(opfc_handle *h, const ColLaunch &L) {
+  return h->prec == OPFC_FP64 ? launch_col<double>(L, h->stream) : launch_col<float>(L, h->stream);
+}
+int xpass(opfc_handle *h, const XLaunch &L) {
+  return h->prec == OPFC_FP64 ? launch_x<double>(L, h->stream) : launch_x<float>(L, h->stream);
+}
+
+// plain batched transform along y/z, in place (in == out) or out of place
+int col_plain(opfc_handle *h, int axis, int dir, const void *in0, void *out0,
+              const void *in1 = nullptr, void *out1 = nullptr) {
+  ColLaunch L{};
+  col_segments(h, axis, L);
+  L.dir = dir;
+  L.mode = COL_PLAIN;
+  L.nsets = in1 ? 2 : 1;
+  L.in[0] = in0;
+  L.out[0] = out0;
+  L.in[1] = in1 ? in1 : in0;
+  L.out[1] = out1 ? out1 : out0;
+  L.tw = axis == 1 ? h->tw_y : h->tw_z;
+  return col(h, L);
+}
+
+XLaunch x_base(opfc_handle *h) {
+  XLaunch L{};
+  L.M = h->M;
+  L.rows = h->n1 * h->n2;
+  L.nyq_off = h->nyq_off;
+  L.tw = h->tw_x;
+  L.scale = 1.0 / ((double)h->n0 * h->n1 * h->n2);
+  L.mean = 0.0;
+  L.flag = h->flag;
+  return L;
+}
+
+double mean_density(const opfc_handle *h) { return h->mass_sum / (double)h->nr; }
+
+// A <- F_z^-1[psi_hat] (and, for TUNGSTEN, B <- F_z^-1[chi psi_hat]); FILTERED
+// keeps only the filtered density in A.
+int prepare_a(opfc_handle *h) {
+  const int model = h->desc.model;
+  if (model == OPFC_MODEL_PLAIN) {
+    LAUNCH_TRY(h, col_plain(h, 2, +1, h->psi_hat, h->work_a));
+  } else {
+    ColLaunch L{};
+    col_segments(h, 2, L);
+    L.mode = COL_PLAIN;
+    L.dir = +1;
+    L.nsets = 1;
+    // psi part (TUNGSTEN) in A
+    if (model == OPFC_MODEL_TUNGSTEN) {
+      L.in[0] = h->psi_hat;
+      L.out[0] = h->work_a;
+      L.in[1] = h->psi_hat;
+      L.out[1] = h->work_a;
+      L.tw = h->tw_z;
+      LAUNCH_TRY(h, col(h, L));
+    }
+    // chi * psi_hat -> scratch, then inverse z
+    void *dst = (model == OPFC_MODEL_TUNGSTEN) ? h->work_b : h->work_a;
+    int rc = opfc_scale_by_table(h, h->psi_hat, h->tab_chi, dst);
+    if (rc) return rc;
+    LAUNCH_TRY(h, col_plain(h, 2, +1, dst, dst));
+  }
+  h->a_valid = true;
+  return OPFC_OK;
+}
+
+// Number of kernels one step launches (YI, X, YF, ZU, HERM).
+constexpr int kStepKernels = 5;
+const char *const kStepKernelNames[kStepKernels] = {"y_inverse", "x_fused", "y_forward",
+                                                     "z_update", "hermitian_fix"};
+
+// Enqueue the step's kernels on h->stream; `only` >= 0 enqueues that one kernel.
+int enqueue_step(opfc_handle *h, int only = -1) {
+  const int model = h->desc.model;
+  if (only < 0 || only == 0) {  // YI
+    if (model == OPFC_MODEL_TUNGSTEN)
+      LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_a, h->work_a, h->work_b, h->work_b));
+    else
+      LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_a, h->work_a));
+  }
+  if (only < 0 || only == 1) {  // X
+    XLaunch X = x_base(h);
+    X.mode = X_FUSED;
+    X.in0 = h->work_a;
+    X.out = h->work_a;
+    X.mean = mean_density(h);
+    if (model == OPFC_MODEL_PLAIN) {
+      X.model = MK_PLAIN;
+    } else if (model == OPFC_MODEL_FILTERED) {
+      X.model = MK_FILTERED;
+      X.c[0] = h->desc.p2 / 2.0;
+      X.c[1] = h->desc.p3 / 3.0;
+      X.c[2] = h->desc.p4 / 4.0;
+    } else {
+      X.model = MK_TUNGSTEN;
+      X.in1 = h->work_b;
+      const opfc_tungsten_params &p = h->desc.tungsten;
+      const double tau = p.T / p.T0;
+      const double p3b = p.shift_u * (p.p3 + 3 * p.shift_s * p.p4);
+      const double p4b = std::pow(p.shift_u, 2) * p.p4;
+      const double q30b = p.shift_u * (p.q30 + 3.0 * p.shift_s * p.q40);
+      const double q31b = p.shift_u * p.q31;
+      const double q40b = std::pow(p.shift_u, 2) * p.q40;
+      X.c[0] = p3b;
+      X.c[1] = p4b;
+      X.c[2] = q31b * tau + q30b;
+      X.c[3] = q40b;
+      X.c[4] = p.stabP;
+    }
+    LAUNCH_TRY(h, xpass(h, X));
+  }
+  if (only < 0 || only == 2)  // YF
+    LAUNCH_TRY(h, col_plain(h, 1, -1, h->work_a, h->work_a));
+  if (only < 0 || only == 3) {  // ZU
+    ColLaunch Z{};
+    col_segments(h, 2, Z);
+    Z.mode = COL_UPDATE;
+    Z.model = model == OPFC_MODEL_PLAIN ? MK_PLAIN : (model == OPFC_MODEL_TUNGSTEN ? MK_TUNGSTEN : MK_FILTERED);
+    Z.inverse_after = 1;
+    Z.nsets = 1;
+    Z.in[0] = h->work_a;
+    Z.out[0] = h->work_a;
+    Z.in[1] = h->work_b;
+    Z.out[1] = h->work_b;
+    Z.tw = h->tw_z;
+    Z.psi_hat = h->psi_hat;
+    Z.tab_a = h->tab_a;
+    Z.tab_b = h->tab_b;
+    Z.tab_chi = h->tab_chi;
+    LAUNCH_TRY(h, col(h, Z));
+  }
+  if (only < 0 || only == 4) {  // Hermitian projection of the kx = 0 / Nyquist planes
+    if (h->prec == OPFC_FP64)
+      LAUNCH_TRY(h, launch_herm_fix<double>(h->psi_hat, h->nyq_off, h->M, h->n1, h->n2, h->stream));
+    else
+      LAUNCH_TRY(h, launch_herm_fix<float>(h->psi_hat, h->nyq_off, h->M, h->n1, h->n2, h->stream));
+  }
+  return OPFC_OK;
+}
+
+void release_graph(opfc_handle *h) {
+  if (h->graph_exec) cudaGraphExecDestroy(h->graph_exec);
+  if (h->graph) cudaGraphDestroy(h->graph);
+  h->graph_exec = nullptr;
+  h->graph = nullptr;
+}
+
+int build_graph(opfc_handle *h) {
+  release_graph(h);
+  CUDA_TRY(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  int rc = enqueue_step(h);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (e != cudaSuccess) return fail(h, OPFC_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  h->graph = g;
+  e = cudaGraphInstantiate(&h->graph_exec, g, 0);
+  if (e != cudaSuccess) {
+    release_graph(h);
+    return fail(h, OPFC_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+  }
+  return OPFC_OK;
+}
+
+int ensure_real_buf(opfc_handle *h) {
+  if (h->real_buf) return OPFC_OK;
+  return dev_alloc(h, &h->real_buf, h->nr * h->rsz);
+}
+
+int check_count(opfc_handle *h, size_t count, size_t expect, const char *what) {
+  if (count != expect)
+    return fail(h, OPFC_ERR_SIZE, "%s: expected %zu elements, got %zu", what, expect, count);
+  return OPFC_OK;
+}
+
+int check_dtype_where(opfc_handle *h, int dtype, int where) {
+  if (dtype != OPFC_F32 && dtype != OPFC_F64) return fail(h, OPFC_ERR_ARG, "bad dtype %d", dtype);
+  if (where != OPFC_HOST && where != OPFC_DEVICE) return fail(h, OPFC_ERR_ARG, "bad location %d", where);
+  return OPFC_OK;
+}
+
+// copy a user real field (any dtype, host or device) into real_buf
+int real_in(opfc_handle *h, const void *src, int dtype, int where) {
+  int rc = ensure_real_buf(h);
+  if (rc) return rc;
+  const bool same = (dtype == OPFC_F64) == (h->prec == OPFC_FP64);
+  if (where == OPFC_HOST) {
+    if (same) {
+      CUDA_TRY(h, cudaMemcpyAsync(h->real_buf, src, h->nr * h->rsz, cudaMemcpyHostToDevice, h->stream));
+    } else if (h->prec == OPFC_FP64) {
+      std::vector<double> tmp(h->nr);
+      const float *f = (const float *)src;
+      for (size_t i = 0; i < h->nr; ++i) tmp[i] = f[i];
+      CUDA_TRY(h, cudaMemcpyAsync(h->real_buf, tmp.data(), h->nr * 8, cudaMemcpyHostToDevice, h->stream));
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    } else {
+      std::vector<float> tmp(h->nr);
+      const double *d = (const double *)src;
+      for (size_t i = 0; i < h->nr; ++i) tmp[i] = (float)d[i];
+      CUDA_TRY(h, cudaMemcpyAsync(h->real_buf, tmp.data(), h->nr * 4, cudaMemcpyHostToDevice, h->stream));
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    }
+  } else {
+    if (same) {
+      CUDA_TRY(h, cudaMemcpyAsync(h->real_buf, src, h->nr * h->rsz, cudaMemcpyDeviceToDevice, h->stream));
+    } else if (h->prec == OPFC_FP64) {
+      LAUNCH_TRY(h, launch_cast_real<double>(src, 0, h->real_buf, 1, h->nr, h->stream));
+    } else {
+      LAUNCH_TRY(h, launch_cast_real<float>(src, 1, h->real_buf, 0, h->nr, h->stream));
+    }
+  }
+  return OPFC_OK;
+}
+
+// copy real_buf out to a user buffer
+int real_out(opfc_handle *h, void *dst, int dtype, int where) {
+  const bool same = (dtype == OPFC_F64) == (h->prec == OPFC_FP64);
+  if (where == OPFC_HOST) {
+    if (same) {
+      CUDA_TRY(h, cudaMemcpyAsync(dst, h->real_buf, h->nr * h->rsz, cudaMemcpyDeviceToHost, h->stream));
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    } else if (h->prec == OPFC_FP64) {
+      std::vector<double> tmp(h->nr);
+      CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), h->real_buf, h->nr * 8, cudaMemcpyDeviceToHost, h->stream));
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+      float *f = (float *)dst;
+      for (size_t i = 0; i < h->nr; ++i) f[i] = (float)tmp[i];
+    } else {
+      std::vector<float> tmp(h->nr);
+      CUDA_TRY(h, cudaMemcpyAsync(tmp.data(), h->real_buf, h->nr * 4, cudaMemcpyDeviceToHost, h->stream));
+      CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+      double *d = (double *)dst;
+      for (size_t i = 0; i < h->nr; ++i) d[i] = tmp[i];
+    }
+  } else {
+    if (same) {
+      CUDA_TRY(h, cudaMemcpyAsync(dst, h->real_buf, h->nr * h->rsz, cudaMemcpyDeviceToDevice, h->stream));
+    } else if (h->prec == OPFC_FP64) {
+      LAUNCH_TRY(h, launch_cast_real<double>(h->real_buf, 1, dst, 0, h->nr, h->stream));
+    } else {
+      LAUNCH_TRY(h, launch_cast_real<float>(h->real_buf, 0, dst, 1, h->nr, h->stream));
+    }
+  }
+  return OPFC_OK;
+}
+
+// compensated FP64 sum of real_buf (p = 1) or of real_buf^4 (p = 4)
+int device_sum(opfc_handle *h, int p, double *out) {
+  if (h->prec == OPFC_FP64)
+    LAUNCH_TRY(h, launch_sum_pow<double>(h->real_buf, h->nr, p, h->partials, h->npartials, h->stream));
+  else
+    LAUNCH_TRY(h, launch_sum_pow<float>(h->real_buf, h->nr, p, h->partials, h->npartials, h->stream));
+  std::vector<double> part(h->npartials);
+  CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->partials, sizeof(double) * h->npartials,
+                              cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  *out = neumaier(part.data(), part.size());
+  return OPFC_OK;
+}
+
+// real_buf -> work_a (forward R2C, full spectrum in the split layout)
+int forward_real_buf(opfc_handle *h, void *dst) {
+  XLaunch X = x_base(h);
+  X.mode = X_R2C;
+  X.rin = h->real_buf;
+  X.out = dst;
+  LAUNCH_TRY(h, xpass(h, X));
+  LAUNCH_TRY(h, col_plain(h, 1, -1, dst, dst));
+  LAUNCH_TRY(h, col_plain(h, 2, -1, dst, dst));
+  return OPFC_OK;
+}
+
+// src (split layout spectrum, z and y not yet inverted) -> real_buf, scaled, + mean
+int backward_to_real_buf(opfc_handle *h, void *src, double mean, bool z_done) {
+  if (!z_done) LAUNCH_TRY(h, col_plain(h, 2, +1, src, src));
+  LAUNCH_TRY(h, col_plain(h, 1, +1, src, src));
+  int rc = ensure_real_buf(h);
+  if (rc) return rc;
+  XLaunch X = x_base(h);
+  X.mode = X_C2R;
+  X.in0 = src;
+  X.rout = h->real_buf;
+  X.mean = mean;
+  LAUNCH_TRY(h, xpass(h, X));
+  return OPFC_OK;
+}
+
+}  // namespace
+
+// elementwise out = psi_hat * table (split layout); used for psi_MF
+__global__ void scale_by_table_f32(const float2 *in, const float *t, float2 *out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float2 v = in[i];
+    const float s = t[i];
+    out[i] = make_float2(v.x * s, v.y * s);
+  }
+}
+__global__ void scale_by_table_f64(const double2 *in, const double *t, double2 *out, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double2 v = in[i];
+    const double s = t[i];
+    out[i] = make_double2(v.x * s, v.y * s);
+  }
+}
+
+int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *out) {
+  const int blocks = 148 * 8;
+  if (h->prec == OPFC_FP64)
+    scale_by_table_f64<<<blocks, 256, 0, h->stream>>>((const double2 *)in, (const double *)tab, (double2 *)out, h->nc);
+  else
+    scale_by_table_f32<<<blocks, 256, 0, h->stream>>>((const float2 *)in, (const float *)tab, (float2 *)out, h->nc);
+  CUDA_TRY(h, cudaGetLastError());
+  return OPFC_OK;
+}
+
+extern "C" {
+
+void opfc_desc_default(opfc_desc *d) {
+  if (!d) return;
+  std::memset(d, 0, sizeof *d);
+  d->n[0] = d->n[1] = d->n[2] = 32;
+  d->dx[0] = d->dx[1] = d->dx[2] = 1.0;
+  d->precision = OPFC_FP32;
+  d->model = OPFC_MODEL_PLAIN;
+  d->r = -0.25;
+  d->filter_alpha = 0.5;
+  d->p2 = -0.1;
+  d->p3 = -0.5;
+  d->p4 = 0.3;
+  opfc_tungsten_params &p = d->tungsten;
+  p.n0 = -0.10; p.n_sol = -0.047; p.n_vap = -0.464; p.T = 3300.0; p.T0 = 156000.0;
+  p.Bx = 0.8582; p.alpha = 0.50; p.alpha_farTol = 0.001; p.alpha_highOrd = 4;
+  p.lambda = 0.22; p.stabP = 0.2; p.shift_u = 0.3341; p.shift_s = 0.1898;
+  p.p2 = 1.0; p.p3 = -0.5; p.p4 = 0.333333333; p.q20 = -0.0037; p.q21 = 1.0;
+  p.q30 = -12.4567; p.q31 = 20.0; p.q40 = 45.0;
+}
+
+const char *opfc_status_string(int s) {
+  switch (s) {
+    case OPFC_OK: return "ok";
+    case OPFC_ERR_ARG: return "invalid argument";
+    case OPFC_ERR_SIZE: return "size contract violated";
+    case OPFC_ERR_CUDA: return "CUDA error";
+    case OPFC_ERR_NONFINITE: return "non-finite value in field";
+    case OPFC_ERR_TIMEOUT: return "device wait timed out";
+    case OPFC_ERR_OOM: return "device out of memory";
+    case OPFC_ERR_STATE: return "call out of order";
+  }
+  return "unknown status";
+}
+
+const char *opfc_last_error(const opfc_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int opfc_destroy(opfc_handle *h) {
+  if (!h) return OPFC_ERR_ARG;
+  int dev_prev = 0;
+  cudaGetDevice(&dev_prev);
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  release_graph(h);
+  void *bufs[] = {h->psi_hat, h->work_a, h->work_b, h->tab_a, h->tab_b, h->tab_chi,
+                  h->tw_x, h->tw_y, h->tw_z, h->real_buf, h->flag, h->partials};
+  for (void *p : bufs)
+    if (p) cudaFree(p);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  cudaSetDevice(dev_prev);
+  delete h;
+  return OPFC_OK;
+}
+
+int opfc_create(const opfc_desc *d, opfc_handle **out) {
+  if (!d || !out) return OPFC_ERR_ARG;
+  *out = nullptr;
+  std::unique_ptr<opfc_handle> h(new opfc_handle);
+  h->desc = *d;
+  if (d->precision != OPFC_FP32 && d->precision != OPFC_FP64) return OPFC_ERR_ARG;
+  if (d->model < OPFC_MODEL_PLAIN || d->model > OPFC_MODEL_FILTERED) return OPFC_ERR_ARG;
+  for (int a = 0; a < 3; ++a)
+    if (d->n[a] < 1 || !(d->dx[a] > 0)) return OPFC_ERR_SIZE;
+  if (d->n[0] < 2 || d->n[0] % 2 != 0) return OPFC_ERR_SIZE;
+  if (!supported_len(d->n[0] / 2) || !supported_len(d->n[1]) || !supported_len(d->n[2]))
+    return OPFC_ERR_SIZE;
+  h->n0 = d->n[0];
+  h->n1 = d->n[1];
+  h->n2 = d->n[2];
+  h->M = h->n0 / 2;
+  h->nr = (size_t)h->n0 * h->n1 * h->n2;
+  h->nc = (size_t)(h->M + 1) * h->n1 * h->n2;
+  h->nyq_off = (long long)h->M * h->n1 * h->n2;
+  h->prec = d->precision;
+  h->rsz = h->prec == OPFC_FP64 ? 8 : 4;
+  h->device = d->device;
+  cudaError_t e = cudaSetDevice(h->device);
+  if (e != cudaSuccess) return OPFC_ERR_CUDA;
+  if (d->stream) {
+    h->stream = (cudaStream_t)d->stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) return OPFC_ERR_CUDA;
+    h->own_stream = true;
+  }
+  const size_t cb = h->nc * 2 * h->rsz;
+  int rc = 0;
+  opfc_handle *hp = h.get();
+  auto cleanup = [&](int code) {
+    opfc_destroy(h.release());
+    return code;
+  };
+  if ((rc = dev_alloc(hp, &hp->psi_hat, cb))) return cleanup(rc);
+  if ((rc = dev_alloc(hp, &hp->work_a, cb))) return cleanup(rc);
+  if (d->model == OPFC_MODEL_TUNGSTEN && (rc = dev_alloc(hp, &hp->work_b, cb))) return cleanup(rc);
+  if ((rc = upload_twiddles(hp, hp->n0, &hp->tw_x))) return cleanup(rc);
+  if ((rc = upload_twiddles(hp, hp->n1, &hp->tw_y))) return cleanup(rc);
+  if ((rc = upload_twiddles(hp, hp->n2, &hp->tw_z))) return cleanup(rc);
+  if ((rc = dev_alloc(hp, (void **)&hp->flag, sizeof(unsigned int)))) return cleanup(rc);
+  if ((rc = dev_alloc(hp, (void **)&hp->partials, sizeof(double) * hp->npartials))) return cleanup(rc);
+  if (cudaMemset(hp->flag, 0, sizeof(unsigned int)) != cudaSuccess) return cleanup(OPFC_ERR_CUDA);
+  if (cudaMemset(hp->psi_hat, 0, cb) != cudaSuccess) return cleanup(OPFC_ERR_CUDA);
+  *out = h.release();
+  return OPFC_OK;
+}
+
+int opfc_initialize(opfc_handle *h, double dt) {
+  if (!h) return OPFC_ERR_ARG;
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(h, OPFC_ERR_ARG, "dt must be positive and finite");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  const int n0 = h->n0, n1 = h->n1, n2 = h->n2, H = h->M + 1;
+  const double f0 = 2.0 * kPi / (h->desc.dx[0] * n0);
+  const double f1 = 2.0 * kPi / (h->desc.dx[1] * n1);
+  const double f2 = 2.0 * kPi / (h->desc.dx[2] * n2);
+  const int model = h->desc.model;
+  const bool need_chi = model != OPFC_MODEL_PLAIN;
+  std::vector<double> ta(h->nc), tb(h->nc), tc(need_chi ? h->nc : 0);
+  auto kc = [](int i, int n, double f) { return (i <= n / 2) ? i * f : (i - n) * f; };
+  const opfc_tungsten_params P = h->desc.tungsten;
+  // Tungsten scalars (tungsten_params.hpp:339-411, tungsten_spectral.hpp:67-75)
+  const double tau = P.T / P.T0;
+  const double p2b = P.p2 + 2 * P.shift_s * P.p3 + 3 * std::pow(P.shift_s, 2) * P.p4;
+  const double q20b = P.q20 + 2.0 * P.shift_s * P.q30 + 3.0 * std::pow(P.shift_s, 2) * P.q40;
+  const double q21b = P.q21 + 2.0 * P.shift_s * P.q31;
+  const double q2b = q21b * tau + q20b;
+  const double alpha2 = 2.0 * P.alpha * P.alpha;
+  const double lambda2 = 2.0 * P.lambda * P.lambda;
+  const double rTol = -alpha2 * std::log(P.alpha_farTol) - 1.0;
+  const double peak = P.Bx * std::exp(-P.T / P.T0);
+  const double r = h->desc.r;
+  const double fa = h->desc.filter_alpha;
+  parallel_for((long)n2 * n1, [&](long row) {
+    const int ky = (int)(row % n1), kz = (int)(row / n1);
+    for (int kx = 0; kx < H; ++kx) {
+      const double kx_ = kc(kx, n0, f0), ky_ = kc(ky, n1, f1), kz_ = kc(kz, n2, f2);
+      const size_t o = split_index(h, kx, ky, kz);
+      if (model == OPFC_MODEL_TUNGSTEN) {
+        // physics_for_mode (tungsten_spectral.hpp:83-104) + spectral_exp_coeffs
+        // (spectral_exp_coefficients.hpp:68-82) + n_weight (tungsten_etd_workspace.hpp:111-130)
+        const double kLap = -((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_));
+        const double fMF = std::exp(kLap / lambda2);
+        const double kv = std::sqrt(-kLap) - 1.0;
+        const double k2 = kv * kv;
+        const double g1 = (P.alpha_highOrd == 0)
+                              ? std::exp(-k2 / alpha2)
+                              : std::exp(-(k2 + rTol * std::pow(kv, P.alpha_highOrd)) / alpha2);
+        const double g2 = 1.0 - 1.0 / alpha2 * k2;
+        const double gf = (kv < 0.0) ? g1 : g2;
+        const double opCk = P.stabP + p2b - peak * gf + q2b * fMF;
+        const double L = kLap * opCk;
+        const double arg = L * dt;
+        const double phi1 = (std::fabs(L) < 1e-12) ? dt + 0.5 * L * dt * dt : std::expm1(arg) / L;
+        ta[o] = std::exp(arg);
+        tb[o] = kLap * phi1;
+        tc[o] = fMF;
+      } else {
+        // 10_complete_pfc_model.cpp:189-207
+        const double k2 = kx_ * kx_ + ky_ * ky_ + kz_ * kz_;
+        const double k2_lap = -k2;
+        const double L = k2_lap * (r + (1.0 - k2) * (1.0 - k2));
+        const double eL = std::exp(L * dt);
+        ta[o] = eL;
+        tb[o] = (std::fabs(L) > 1e-14) ? (eL - 1.0) / L * k2_lap : dt * k2_lap;
+        if (need_chi) tc[o] = std::exp(-k2 / (2.0 * fa * fa));
+      }
+    }
+  });
+  auto upload = [&](std::vector<double> &src, void **dst) -> int {
+    if (!*dst) {
+      int rc = dev_alloc(h, dst, h->nc * h->rsz);
+      if (rc) return rc;
+    }
+    if (h->prec == OPFC_FP64) {
+      CUDA_TRY(h, cudaMemcpy(*dst, src.data(), h->nc * 8, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(src.begin(), src.end());
+      CUDA_TRY(h, cudaMemcpy(*dst, f.data(), h->nc * 4, cudaMemcpyHostToDevice));
+    }
+    return OPFC_OK;
+  };
+  int rc;
+  if ((rc = upload(ta, &h->tab_a))) return rc;
+  if ((rc = upload(tb, &h->tab_b))) return rc;
+  if (need_chi && (rc = upload(tc, &h->tab_chi))) return rc;
+  h->dt = dt;
+  h->initialized = true;
+  h->a_valid = false;
+  release_graph(h);
+  return OPFC_OK;
+}
+
+int opfc_set_psi(opfc_handle *h, const void *psi, size_t count, int dtype, int where) {
+  if (!h || !psi) return h ? fail(h, OPFC_ERR_ARG, "null field pointer") : OPFC_ERR_ARG;
+  int rc;
+  if ((rc = check_dtype_where(h, dtype, where))) return rc;
+  if ((rc = check_count(h, count, h->nr, "opfc_set_psi"))) return rc;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  if ((rc = real_in(h, psi, dtype, where))) return rc;
+  // k = 0 mode in FP64 with compensated summation (of the values as stored in
+  // the compute precision, so the mean is that of the field actually evolved)
+  if ((rc = device_sum(h, 1, &h->mass_sum))) return rc;
+  if ((rc = forward_real_buf(h, h->psi_hat))) return rc;
+  // the DC slot of the FP32/FP64 array stays zero; mass_sum carries it
+  CUDA_TRY(h, cudaMemsetAsync(h->psi_hat, 0, 2 * h->rsz, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  h->have_state = true;
+  h->a_valid = false;
+  release_graph(h);  // the captured step bakes in the mean density
+  return OPFC_OK;
+}
+
+int opfc_get_psi(opfc_handle *h, void *psi, size_t count, int dtype, int where) {
+  if (!h || !psi) return h ? fail(h, OPFC_ERR_ARG, "null field pointer") : OPFC_ERR_ARG;
+  int rc;
+  if ((rc = check_dtype_where(h, dtype, where))) return rc;
+  if ((rc = check_count(h, count, h->nr, "opfc_get_psi"))) return rc;
+  if (!h->have_state) return fail(h, OPFC_ERR_STATE, "opfc_get_psi before opfc_set_psi");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  LAUNCH_TRY(h, col_plain(h, 2, +1, h->psi_hat, h->work_a));
+  if ((rc = backward_to_real_buf(h, h->work_a, mean_density(h), true))) return rc;
+  h->a_valid = false;
+  return real_out(h, psi, dtype, where);
+}
+
+int opfc_get_psi_mf(opfc_handle *h, void *psi, size_t count, int dtype, int where) {
+  if (!h || !psi) return h ? fail(h, OPFC_ERR_ARG, "null field pointer") : OPFC_ERR_ARG;
+  int rc;
+  if ((rc = check_dtype_where(h, dtype, where))) return rc;
+  if ((rc = check_count(h, count, h->nr, "opfc_get_psi_mf"))) return rc;
+  if (!h->have_state || !h->initialized) return fail(h, OPFC_ERR_STATE, "need state and tables");
+  if (!h->tab_chi) return fail(h, OPFC_ERR_STATE, "model has no mean-field filter");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  if ((rc = opfc_scale_by_table(h, h->psi_hat, h->tab_chi, h->work_a))) return rc;
+  // chi(0) = 1 in every model, so the mean carries over unchanged
+  if ((rc = backward_to_real_buf(h, h->work_a, mean_density(h), false))) return rc;
+  h->a_valid = false;
+  return real_out(h, psi, dtype, where);
+}
+
+int opfc_get_psi_hat(opfc_handle *h, void *out, size_t count, int dtype, int where) {
+  if (!h || !out) return h ? fail(h, OPFC_ERR_ARG, "null pointer") : OPFC_ERR_ARG;
+  int rc;
+  if ((rc = check_dtype_where(h, dtype, where))) return rc;
+  if ((rc = check_count(h, count, h->nc, "opfc_get_psi_hat"))) return rc;
+  if (!h->have_state) return fail(h, OPFC_ERR_STATE, "opfc_get_psi_hat before opfc_set_psi");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  const size_t esz = dtype == OPFC_F64 ? 8 : 4;
+  void *dst = out;
+  void *tmp = nullptr;
+  if (where == OPFC_HOST) {
+    CUDA_TRY(h, cudaMallocAsync(&tmp, h->nc * 2 * esz, h->stream));
+    dst = tmp;
+  }
+  const int f64 = dtype == OPFC_F64;
+  if (h->prec == OPFC_FP64)
+    rc = launch_to_ref<double>(h->psi_hat, dst, f64, h->M, h->n1, h->n2, h->nyq_off, 1, h->mass_sum, h->stream);
+  else
+    rc = launch_to_ref<float>(h->psi_hat, dst, f64, h->M, h->n1, h->n2, h->nyq_off, 1, h->mass_sum, h->stream);
+  if (rc) return fail(h, OPFC_ERR_CUDA, "to_ref: %s", cudaGetErrorString((cudaError_t)rc));
+  if (tmp) {
+    CUDA_TRY(h, cudaMemcpyAsync(out, tmp, h->nc * 2 * esz, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaFreeAsync(tmp, h->stream));
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return OPFC_OK;
+}
+
+int opfc_step(opfc_handle *h, int n_steps) {
+  if (!h) return OPFC_ERR_ARG;
+  if (n_steps < 0) return fail(h, OPFC_ERR_ARG, "negative step count");
+  if (!h->initialized) return fail(h, OPFC_ERR_STATE, "opfc_step before opfc_initialize");
+  if (!h->have_state) return fail(h, OPFC_ERR_STATE, "opfc_step before opfc_set_psi");
+  if (n_steps == 0) return OPFC_OK;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  int rc;
+  if (!h->a_valid && (rc = prepare_a(h))) return rc;
+  if (!h->graph_exec) {
+    if ((rc = build_graph(h))) return rc;
+  }
+  for (int s = 0; s < n_steps; ++s) CUDA_TRY(h, cudaGraphLaunch(h->graph_exec, h->stream));
+  return OPFC_OK;
+}
+
+int opfc_sync(opfc_handle *h) {
+  if (!h) return OPFC_ERR_ARG;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  unsigned int f = 0;
+  CUDA_TRY(h, cudaMemcpy(&f, h->flag, sizeof f, cudaMemcpyDeviceToHost));
+  if (f) {
+    cudaMemset(h->flag, 0, sizeof f);
+    return fail(h, OPFC_ERR_NONFINITE, "non-finite value produced by the nonlinearity");
+  }
+  return OPFC_OK;
+}
+
+int opfc_fft_forward(opfc_handle *h, const void *in_real, void *out_complex, int dtype, int where) {
+  if (!h || !in_real || !out_complex) return h ? fail(h, OPFC_ERR_ARG, "null pointer") : OPFC_ERR_ARG;
+  int rc;
+  if ((rc = check_dtype_where(h, dtype, where))) return rc;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  if ((rc = real_in(h, in_real, dtype, where))) return rc;
+  if ((rc = forward_real_buf(h, h->work_a))) return rc;
+  h->a_valid = false;
+  const size_t esz = dtype == OPFC_F64 ? 8 : 4;
+  void *dst = out_complex, *tmp = nullptr;
+  if (where == OPFC_HOST) {
+    CUDA_TRY(h, cudaMallocAsync(&tmp, h->nc * 2 * esz, h->stream));
+    dst = tmp;
+  }
+  const int f64 = dtype == OPFC_F64;
+  if (h->prec == OPFC_FP64)
+    rc = launch_to_ref<double>(h->work_a, dst, f64, h->M, h->n1, h->n2, h->nyq_off, 0, 0.0, h->stream);
+  else
+    rc = launch_to_ref<float>(h->work_a, dst, f64, h->M, h->n1, h->n2, h->nyq_off, 0, 0.0, h->stream);
+  if (rc) return fail(h, OPFC_ERR_CUDA, "to_ref: %s", cudaGetErrorString((cudaError_t)rc));
+  if (tmp) {
+    CUDA_TRY(h, cudaMemcpyAsync(out_complex, tmp, h->nc * 2 * esz, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaFreeAsync(tmp, h->stream));
+  }
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return OPFC_OK;
+}
+
+int opfc_fft_backward(opfc_handle *h, const void *in_complex, void *out_real, int dtype, int where) {
+  if (!h || !in_complex || !out_real) return h ? fail(h, OPFC_ERR_ARG, "null pointer") : OPFC_ERR_ARG;
+  int rc;
+  if ((rc = check_dtype_where(h, dtype, where))) return rc;
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  const size_t esz = dtype == OPFC_F64 ? 8 : 4;
+  const void *src = in_complex;
+  void *tmp = nullptr;
+  if (where == OPFC_HOST) {
+    CUDA_TRY(h, cudaMallocAsync(&tmp, h->nc * 2 * esz, h->stream));
+    CUDA_TRY(h, cudaMemcpyAsync(tmp, in_complex, h->nc * 2 * esz, cudaMemcpyHostToDevice, h->stream));
+    src = tmp;
+  }
+  const int f64 = dtype == OPFC_F64;
+  if (h->prec == OPFC_FP64)
+    rc = launch_from_ref<double>(src, f64, h->work_a, h->M, h->n1, h->n2, h->nyq_off, h->stream);
+  else
+    rc = launch_from_ref<float>(src, f64, h->work_a, h->M, h->n1, h->n2, h->nyq_off, h->stream);
+  if (rc) return fail(h, OPFC_ERR_CUDA, "from_ref: %s", cudaGetErrorString((cudaError_t)rc));
+  if (tmp) CUDA_TRY(h, cudaFreeAsync(tmp, h->stream));
+  h->a_valid = false;
+  if ((rc = backward_to_real_buf(h, h->work_a, 0.0, false))) return rc;
+  return real_out(h, out_real, dtype, where);
+}
+
+int opfc_mass(opfc_handle *h, double *mean) {
+  if (!h || !mean) return OPFC_ERR_ARG;
+  if (!h->have_state) return fail(h, OPFC_ERR_STATE, "no state");
+  *mean = mean_density(h);
+  return OPFC_OK;
+}
+
+int opfc_free_energy(opfc_handle *h, double *energy) {
+  if (!h || !energy) return OPFC_ERR_ARG;
+  if (!h->have_state) return fail(h, OPFC_ERR_STATE, "no state");
+  if (h->desc.model == OPFC_MODEL_TUNGSTEN)
+    return fail(h, OPFC_ERR_ARG, "free energy is defined for the plain and filtered models");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  // quadratic part by Parseval in k-space (FP64 accumulation of the resident state)
+  if (h->prec == OPFC_FP64)
+    LAUNCH_TRY(h, launch_energy_k<double>(h->psi_hat, h->M, h->n1, h->n2, h->nyq_off, h->desc.dx,
+                                          h->desc.r, h->partials, h->npartials, h->stream));
+  else
+    LAUNCH_TRY(h, launch_energy_k<float>(h->psi_hat, h->M, h->n1, h->n2, h->nyq_off, h->desc.dx,
+                                         h->desc.r, h->partials, h->npartials, h->stream));
+  std::vector<double> part(h->npartials);
+  CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->partials, sizeof(double) * h->npartials,
+                              cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  double sk = neumaier(part.data(), part.size());
+  sk += (h->desc.r + 1.0) * h->mass_sum * h->mass_sum;  // k = 0 mode, G(0) = r + 1
+  // quartic part in real space
+  int rc;
+  LAUNCH_TRY(h, col_plain(h, 2, +1, h->psi_hat, h->work_a));
+  if ((rc = backward_to_real_buf(h, h->work_a, mean_density(h), true))) return rc;
+  h->a_valid = false;
+  double s4 = 0;
+  if ((rc = device_sum(h, 4, &s4))) return rc;
+  const double dV = h->desc.dx[0] * h->desc.dx[1] * h->desc.dx[2];
+  *energy = dV * (0.5 * sk / (double)h->nr + 0.25 * s4);
+  return OPFC_OK;
+}
+
+size_t opfc_size_inbox(const opfc_handle *h) { return h ? h->nr : 0; }
+size_t opfc_size_outbox(const opfc_handle *h) { return h ? h->nc : 0; }
+size_t opfc_allocated_bytes(const opfc_handle *h) { return h ? h->allocated : 0; }
+void *opfc_get_stream(const opfc_handle *h) { return h ? (void *)h->stream : nullptr; }
+int opfc_kernels_per_step(const opfc_handle *h) { return h ? kStepKernels : 0; }
+
+int opfc_profile_step(opfc_handle *h, int reps, double *ms, int max_kernels) {
+  if (!h || !ms || reps < 1) return OPFC_ERR_ARG;
+  if (!h->initialized || !h->have_state) return fail(h, OPFC_ERR_STATE, "profile needs tables and a state");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  int rc;
+  if (!h->a_valid && (rc = prepare_a(h))) return rc;
+  cudaEvent_t e0, e1;
+  CUDA_TRY(h, cudaEventCreate(&e0));
+  CUDA_TRY(h, cudaEventCreate(&e1));
+  const int nk = std::min(max_kernels, kStepKernels);
+  for (int k = 0; k < nk; ++k) {
+    // one untimed launch, then `reps` timed launches of kernel k alone
+    if ((rc = enqueue_step(h, k))) break;
+    cudaEventRecord(e0, h->stream);
+    for (int r = 0; r < reps && !rc; ++r) rc = enqueue_step(h, k);
+    cudaEventRecord(e1, h->stream);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    ms[k] = (double)t / reps;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // the repeated in-place passes leave the field undefined
+  h->have_state = false;
+  h->a_valid = false;
+  cudaMemset(h->flag, 0, sizeof(unsigned int));
+  if (rc) return rc;
+  return nk;
+}
+
+// ---------------------------------------------------------------------------
+// initial conditions (host; set-up only).  Cells in x-fastest order
+// (include/openpfc/kernel/field/operations.hpp:96-103), one 64-bit draw of
+// std::mt19937_64 per random number, u = (draw >> 11) * 2^-53.
+// ---------------------------------------------------------------------------
+static inline double mt_unit(std::mt19937_64 &g) { return (double)(g() >> 11) * (1.0 / 9007199254740992.0); }
+
+int opfc_ic_noise(double *psi, size_t count, double n0, double amp, uint64_t seed) {
+  if (!psi) return OPFC_ERR_ARG;
+  std::mt19937_64 g(seed);
+  for (size_t i = 0; i < count; ++i) psi[i] = n0 + (-amp + 2.0 * amp * mt_unit(g));
+  return OPFC_OK;
+}
+
+// One-mode BCC seed of the reference (single_seed.hpp, seed.hpp): six
+// <110>/sqrt(2) vectors, u = rho + sum_q 2 amp cos(q.x) for |x - c| < radius.
+static const double kQ[6][3] = {{1, 1, 0}, {1, 0, 1}, {0, 1, 1}, {1, 0, -1}, {1, -1, 0}, {0, 1, -1}};
+
+int opfc_ic_seed(double *psi, const int n[3], const double dx[3], const double origin[3],
+                 const double center[3], double radius, double rho, double amp, int outside_zero) {
+  if (!psi || !n || !dx || !origin || !center) return OPFC_ERR_ARG;
+  const double s = 1.0 / std::sqrt(2.0);
+  const double r2 = std::pow(radius, 2);
+  size_t idx = 0;
+  for (int k = 0; k < n[2]; ++k)
+    for (int j = 0; j < n[1]; ++j)
+      for (int i = 0; i < n[0]; ++i, ++idx) {
+        const double x = origin[0] + i * dx[0] - center[0];
+        const double y = origin[1] + j * dx[1] - center[1];
+        const double z = origin[2] + k * dx[2] - center[2];
+        if (x * x + y * y + z * z < r2) {
+          double u = rho;
+          for (int q = 0; q < 6; ++q)
+            u += 2.0 * amp * std::cos(s * kQ[q][0] * x + s * kQ[q][1] * y + s * kQ[q][2] * z);
+          psi[idx] = u;
+        } else if (outside_zero) {
+          psi[idx] = 0.0;
+        }
+      }
+  return OPFC_OK;
+}
+
+int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, double noise,
+                  int nseeds, double radius_cells, double amp, uint64_t seed) {
+  if (!psi || !n || !dx || nseeds < 0) return OPFC_ERR_ARG;
+  const size_t ncell = (size_t)n[0] * n[1] * n[2];
+  std::mt19937_64 g(seed);
+  for (size_t i = 0; i < ncell; ++i) psi[i] = n0 + (-noise + 2.0 * noise * mt_unit(g));
+  const double s = 1.0 / std::sqrt(2.0);
+  for (int sd = 0; sd < nseeds; ++sd) {
+    double c[3];
+    for (int a = 0; a < 3; ++a) c[a] = mt_unit(g) * n[a];
+    const double R2 = radius_cells * radius_cells;
+    size_t idx = 0;
+    for (int k = 0; k < n[2]; ++k)
+      for (int j = 0; j < n[1]; ++j)
+        for (int i = 0; i < n[0]; ++i, ++idx) {
+          double d[3] = {i - c[0], j - c[1], k - c[2]};
+          for (int a = 0; a < 3; ++a) {  // periodic minimum image
+            if (d[a] > 0.5 * n[a]) d[a] -= n[a];
+            if (d[a] < -0.5 * n[a]) d[a] += n[a];
+          }
+          if (d[0] * d[0] + d[1] * d[1] + d[2] * d[2] >= R2) continue;
+          const double X = d[0] * dx[0], Y = d[1] * dx[1], Z = d[2] * dx[2];
+          double u = n0;
+          for (int q = 0; q < 6; ++q) u += amp * std::cos(s * kQ[q][0] * X + s * kQ[q][1] * Y + s * kQ[q][2] * Z);
+          psi[idx] = u;
+        }
+  }
+  return OPFC_OK;
+}
+
+const char *opfc_step_kernel_name(int k) {
+  return (k >= 0 && k < kStepKernels) ? kStepKernelNames[k] : "";
+}
+
+}  // extern "C"
