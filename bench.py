@@ -68,25 +68,38 @@ class Clocks:
         self.p = None
 
     def __enter__(self):
+        import threading
+        self.lines = []
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                        "-i", str(self.device), "-lms", "100"],
                                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
+            return self
+
+        def reader():
+            for line in self.p.stdout:
+                if line.strip():
+                    self.lines.append(line)
+
+        self.t = threading.Thread(target=reader, daemon=True)
+        self.t.start()
+        t0 = time.time()
+        while not self.lines and time.time() - t0 < 3.0:  # first sample before the region
+            time.sleep(0.01)
+        self.lines.clear()
         return self
 
     def __exit__(self, *a):
-        self.lines = []
         if self.p:
-            time.sleep(0.25)
+            time.sleep(0.15)
             self.p.terminate()
             try:
-                out, _ = self.p.communicate(timeout=5)
+                self.p.wait(timeout=5)
             except Exception:
                 self.p.kill()
-                out = ""
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.t.join(timeout=2)
 
     def summary(self):
         sm, smax, reasons = [], None, set()
@@ -204,6 +217,7 @@ def run_b200(args):
     m.initialize(DT)
     m.set_psi(psi0_32)
     stream = torch.cuda.ExternalStream(m.stream, device=torch.device("cuda", local))
+    # clocks are sampled from the warm-up through the end of the timed region
     with Clocks(local) as ck:
         ms = timed_steps(m, args.steps, args.warmup, ws, stream)
     value = ws * cells * args.steps / (ms / 1e3) / 1e6
@@ -311,7 +325,9 @@ def run_b200(args):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--n", type=int, default=512,
+                    help="grid side (512 is the measured workload; smaller sides are for profiling)")
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-fp64", action="store_true")
@@ -321,6 +337,10 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
+    global N, WORKLOAD
+    if args.n != N:
+        WORKLOAD = WORKLOAD.replace(f"{N}^3", f"{args.n}^3")
+        N = args.n
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

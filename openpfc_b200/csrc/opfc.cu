@@ -87,7 +87,7 @@ double neumaier(const double *a, size_t n) {
 
 template <typename F> void parallel_for(long n, F &&f) {
   unsigned nt = std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
-  if (n < 4096) nt = 1;
+  if ((long)nt > n) nt = (unsigned)std::max(1L, n);
   std::vector<std::thread> th;
   const long chunk = (n + nt - 1) / nt;
   for (unsigned t = 0; t < nt; ++t) {
@@ -509,6 +509,39 @@ int device_sum(opfc_handle *h, int p, double *out) {
   return OPFC_OK;
 }
 
+// Compensated FP64 sum of a user field (host: threaded Neumaier chunks
+// combined with Neumaier; device: the FP64 reduction kernel in the field's dtype).
+int user_sum(opfc_handle *h, const void *src, int dtype, int where, double *out) {
+  if (where == OPFC_DEVICE) {
+    if (dtype == OPFC_F64)
+      LAUNCH_TRY(h, launch_sum_pow<double>(src, h->nr, 1, h->partials, h->npartials, h->stream));
+    else
+      LAUNCH_TRY(h, launch_sum_pow<float>(src, h->nr, 1, h->partials, h->npartials, h->stream));
+    std::vector<double> part(h->npartials);
+    CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->partials, sizeof(double) * h->npartials,
+                                cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    *out = neumaier(part.data(), part.size());
+    return OPFC_OK;
+  }
+  const long nchunk = 64;
+  const size_t len = (h->nr + nchunk - 1) / nchunk;
+  std::vector<double> part(nchunk, 0.0);
+  parallel_for(nchunk, [&](long c) {
+    const size_t lo = (size_t)c * len, hi = std::min(h->nr, lo + len);
+    double s = 0, comp = 0;
+    for (size_t i = lo; i < hi; ++i) {
+      const double v = dtype == OPFC_F64 ? ((const double *)src)[i] : (double)((const float *)src)[i];
+      const double t = s + v;
+      comp += (std::fabs(s) >= std::fabs(v)) ? (s - t) + v : (v - t) + s;
+      s = t;
+    }
+    part[c] = s + comp;
+  });
+  *out = neumaier(part.data(), part.size());
+  return OPFC_OK;
+}
+
 // real_buf -> work_a (forward R2C, full spectrum in the split layout)
 int forward_real_buf(opfc_handle *h, void *dst) {
   XLaunch X = x_base(h);
@@ -762,9 +795,9 @@ int opfc_set_psi(opfc_handle *h, const void *psi, size_t count, int dtype, int w
   if ((rc = check_count(h, count, h->nr, "opfc_set_psi"))) return rc;
   CUDA_TRY(h, cudaSetDevice(h->device));
   if ((rc = real_in(h, psi, dtype, where))) return rc;
-  // k = 0 mode in FP64 with compensated summation (of the values as stored in
-  // the compute precision, so the mean is that of the field actually evolved)
-  if ((rc = device_sum(h, 1, &h->mass_sum))) return rc;
+  // k = 0 mode in FP64 with compensated summation of the caller's values in
+  // their own precision (before any rounding to the compute precision)
+  if ((rc = user_sum(h, psi, dtype, where, &h->mass_sum))) return rc;
   if ((rc = forward_real_buf(h, h->psi_hat))) return rc;
   // the DC slot of the FP32/FP64 array stays zero; mass_sum carries it
   CUDA_TRY(h, cudaMemsetAsync(h->psi_hat, 0, 2 * h->rsz, h->stream));
