@@ -1,0 +1,304 @@
+// col_tma.cuh -- persistent, TMA-fed column passes (y and z transforms, and
+// the fused z transform + ETD update).
+//
+// Each CTA owns one SM and walks the tiles t = blockIdx.x + i * gridDim.x.  A
+// tile is W adjacent columns x N rows of one strided axis; it arrives in shared
+// memory through cp.async.bulk.tensor (no multicast) and is consumed from an
+// mbarrier-guarded ring of STAGES buffers, so the loads of the next tiles are in
+// flight while the current tile is transformed.  The shared tile [p][c] (pitch
+// W, c fastest) is also the FFT's exchange buffer.  For the ETD update the state
+// psi_hat and the operator tables of the same tile ride in the same stage.
+// Every wait is bounded (4 s of globaltimer); on expiry the CTA records
+// OPFC timeout bit 2 in `flag`, drains its own loads (bounded) and leaves.
+#pragma once
+#include <cuda.h>
+
+#include "fft_core.cuh"
+
+namespace opfc {
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Wait for phase `parity` of `bar`; false after ~4 s.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+  const unsigned a = smem_u32(bar);
+  unsigned long long t0 = 0;
+  for (unsigned i = 0;; ++i) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (i == 0)
+      t0 = global_ns();
+    else if ((i & 31u) == 0 && global_ns() - t0 > 4000000000ull)
+      return false;
+  }
+}
+
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x,
+                                            int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
+      : "memory");
+}
+
+constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
+constexpr int kMaxDynSmem = 232448;  // 227 KB opt-in per CTA on sm_100
+
+template <typename Real, int N, int W, int MODE, int MODEL> struct TmaCfg {
+  using C = typename Cx<Real>::T;
+  static constexpr bool UPD = MODE == COL_UPDATE;
+  static constexpr bool CHI = UPD && MODEL != MK_PLAIN;
+  static constexpr size_t TILE_C = size_t(N) * W * sizeof(C);
+  static constexpr size_t TILE_R = size_t(N) * W * sizeof(Real);
+  static constexpr size_t STAGE = TILE_C + (UPD ? TILE_C + 2 * TILE_R + (CHI ? TILE_R : 0) : 0);
+  static constexpr size_t TW = align128(size_t(N) * sizeof(C));
+  static constexpr int S0 = int((kMaxDynSmem - TW - 128) / STAGE);
+  static constexpr int STAGES = S0 > 3 ? 3 : S0;
+  static constexpr size_t SMEM = TW + size_t(STAGES > 0 ? STAGES : 1) * STAGE + 64;
+  static constexpr int RB = N < 256 ? N : 256;  // rows per TMA box (box dims <= 256)
+  static constexpr int NB = N / RB;
+};
+
+// Tensor maps: PLAIN uses m0 (array set 0) and m1 (array set 1); UPDATE uses
+// m0 = N_hat partial (A), m1 = psi_hat, m2 = tab_a, m3 = tab_b, m4 = tab_chi.
+template <typename Real, int N, int W, int MODE, int DIR, int MODEL, bool INV>
+__global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
+    col_tma_kernel(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
+                   const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3,
+                   const __grid_constant__ CUtensorMap m4, const ColArgs<Real> a, const int axis,
+                   unsigned *flag) {
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL>;
+  using C = typename Cx<Real>::T;
+  constexpr int E = Plan<N>::E;
+  constexpr int T = N / E;
+  constexpr int NT = W * T;
+  constexpr int STAGES = Cfg::STAGES;
+  constexpr bool UPD = Cfg::UPD;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  unsigned char *stage0 = smraw + Cfg::TW;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(stage0 + STAGES * Cfg::STAGE);
+
+  const int tid = threadIdx.x;
+  const int c = tid % W;
+  const int j = tid / W;
+  const C *gtw = reinterpret_cast<const C *>(a.tw);
+  for (int i = tid; i < N; i += NT) tw[i] = gtw[i];
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  const int set = blockIdx.y;
+  const CUtensorMap *min = (MODE == COL_PLAIN && set == 1) ? &m1 : &m0;
+  const ColSeg sg = a.seg0;
+  const int ntm = sg.ntiles;
+  const int G = gridDim.x;
+
+  auto issue = [&](int s, int t) {
+    const int ti = t % sg.tiles_inner, to = t / sg.tiles_inner;
+    unsigned char *st = stage0 + s * Cfg::STAGE;
+    mbar_expect_tx(&bars[s], (unsigned)Cfg::STAGE);
+#pragma unroll
+    for (int b = 0; b < Cfg::NB; ++b) {
+      const int r0 = b * Cfg::RB;
+      const int y = axis == 1 ? r0 : to, z = axis == 1 ? to : r0;
+      const size_t offc = size_t(b) * Cfg::RB * W * sizeof(C);
+      tma_load_3d(st + offc, min, &bars[s], ti * W * 2, y, z);
+      if constexpr (UPD) {
+        const size_t offr = size_t(b) * Cfg::RB * W * sizeof(Real);
+        tma_load_3d(st + Cfg::TILE_C + offc, &m1, &bars[s], ti * W * 2, y, z);
+        tma_load_3d(st + 2 * Cfg::TILE_C + offr, &m2, &bars[s], ti * W, y, z);
+        tma_load_3d(st + 2 * Cfg::TILE_C + Cfg::TILE_R + offr, &m3, &bars[s], ti * W, y, z);
+        if constexpr (Cfg::CHI)
+          tma_load_3d(st + 2 * Cfg::TILE_C + 2 * Cfg::TILE_R + offr, &m4, &bars[s], ti * W, y, z);
+      }
+    }
+  };
+
+  if (tid == 0)
+    for (int s = 0; s < STAGES; ++s) {
+      const int t = blockIdx.x + s * G;
+      if (t < ntm) issue(s, t);
+    }
+
+  const C *gin = reinterpret_cast<const C *>(a.in[set]);
+  C *gout = reinterpret_cast<C *>(a.out[set]);
+  (void)gin;
+  int it = 0;
+  bool alive = true;
+  for (int t = blockIdx.x; t < ntm; t += G, ++it) {
+    const int s = it % STAGES;
+    const unsigned par = (unsigned)(it / STAGES) & 1u;
+    const bool ok = mbar_wait(&bars[s], par);
+    if (!__syncthreads_and(ok)) {
+      alive = false;
+      break;
+    }
+    unsigned char *st = stage0 + s * Cfg::STAGE;
+    C *tin = reinterpret_cast<C *>(st);
+    const int ti = t % sg.tiles_inner, to = t / sg.tiles_inner;
+    const long long base =
+        sg.off + (long long)to * sg.s_outer + (long long)(ti * W + c) * sg.col_stride;
+    const long long fs = sg.fft_stride;
+    C v[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = tin[(j + T * m) * W + c];
+    __syncthreads();
+    if constexpr (MODE == COL_PLAIN) {
+      fft_line<C, N, DIR, N>(v, tin, W, c, j, tw);
+#pragma unroll
+      for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
+    } else {
+      fft_line<C, N, -1, N>(v, tin, W, c, j, tw);
+      const C *tpsi = reinterpret_cast<const C *>(st + Cfg::TILE_C);
+      const Real *ta = reinterpret_cast<const Real *>(st + 2 * Cfg::TILE_C);
+      const Real *tb = ta + N * W;
+      const Real *tc = tb + N * W;
+      C *ph = reinterpret_cast<C *>(a.psi_hat);
+      C w[Cfg::CHI ? E : 1];
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const int e = (j + T * m) * W + c;
+        const C p = tpsi[e];
+        const Real la = ta[e], lb = tb[e];
+        const C np = mk<C>(la * p.x + lb * v[m].x, la * p.y + lb * v[m].y);
+        ph[base + (long long)(j + T * m) * fs] = np;
+        if constexpr (Cfg::CHI) w[m] = cscale(np, tc[e]);
+        v[m] = np;
+      }
+      if constexpr (INV) {
+        if constexpr (MODEL == MK_FILTERED) {
+          fft_line<C, N, +1, N>(w, tin, W, c, j, tw);
+#pragma unroll
+          for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = w[m];
+        } else {
+          fft_line<C, N, +1, N>(v, tin, W, c, j, tw);
+#pragma unroll
+          for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
+          if constexpr (MODEL == MK_TUNGSTEN) {
+            C *gout2 = reinterpret_cast<C *>(a.out[1]);
+            fft_line<C, N, +1, N>(w, tin, W, c, j, tw);
+#pragma unroll
+            for (int m = 0; m < E; ++m) gout2[base + (long long)(j + T * m) * fs] = w[m];
+          }
+        }
+      }
+    }
+    // the stage's buffers were read and (as exchange space) written by the
+    // generic proxy; order that before the next asynchronous fill
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      const int tn = t + STAGES * G;
+      if (tn < ntm) issue(s, tn);
+    }
+  }
+
+  if (!alive) {
+    if (tid == 0) atomicOr(flag, 2u);
+    // drain the loads this CTA still has in flight (bounded), then leave
+    const int mine = (ntm - (int)blockIdx.x + G - 1) / G;
+    const int issued = mine < it + STAGES ? mine : it + STAGES;
+    for (int k = it; k < issued; ++k) mbar_wait(&bars[k % STAGES], (unsigned)(k / STAGES) & 1u);
+    return;
+  }
+
+  // Nyquist-plane tiles: direct loads, stage 0 as the exchange buffer
+  const ColSeg sn = a.seg1;
+  C *sm = reinterpret_cast<C *>(stage0);
+  for (int t = blockIdx.x; t < sn.ntiles; t += G) {
+    const int ti = t % sn.tiles_inner, to = t / sn.tiles_inner;
+    const int cg = ti * W + c;
+    const bool ok = cg < sn.ncols;
+    const long long base = sn.off + (long long)to * sn.s_outer + (long long)cg * sn.col_stride;
+    const long long fs = sn.fft_stride;
+    const C *in = reinterpret_cast<const C *>(a.in[set]);
+    C v[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = ok ? in[base + (long long)(j + T * m) * fs] : mk<C>(0, 0);
+    if constexpr (MODE == COL_PLAIN) {
+      fft_line<C, N, DIR, N>(v, sm, W, c, j, tw);
+      if (ok) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
+      }
+    } else {
+      fft_line<C, N, -1, N>(v, sm, W, c, j, tw);
+      C *ph = reinterpret_cast<C *>(a.psi_hat);
+      C w[Cfg::CHI ? E : 1];
+#pragma unroll
+      for (int m = 0; m < E; ++m) {
+        const long long idx = base + (long long)(j + T * m) * fs;
+        C np = mk<C>(0, 0);
+        if (ok) {
+          const C p = ph[idx];
+          const Real la = a.tab_a[idx], lb = a.tab_b[idx];
+          np = mk<C>(la * p.x + lb * v[m].x, la * p.y + lb * v[m].y);
+          ph[idx] = np;
+        }
+        if constexpr (Cfg::CHI) w[m] = ok ? cscale(np, a.tab_chi[idx]) : mk<C>(0, 0);
+        v[m] = np;
+      }
+      if constexpr (INV) {
+        if constexpr (MODEL == MK_FILTERED) {
+          fft_line<C, N, +1, N>(w, sm, W, c, j, tw);
+          if (ok) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = w[m];
+          }
+        } else {
+          fft_line<C, N, +1, N>(v, sm, W, c, j, tw);
+          if (ok) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
+          }
+          if constexpr (MODEL == MK_TUNGSTEN) {
+            C *gout2 = reinterpret_cast<C *>(a.out[1]);
+            fft_line<C, N, +1, N>(w, sm, W, c, j, tw);
+            if (ok) {
+#pragma unroll
+              for (int m = 0; m < E; ++m) gout2[base + (long long)(j + T * m) * fs] = w[m];
+            }
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace opfc

@@ -33,6 +33,11 @@ template <typename Real> struct ColArgs {
 };
 
 template <typename C> __device__ __forceinline__ C czero() { return mk<C>(0, 0); }
+}  // namespace opfc
+
+#include "col_tma.cuh"
+
+namespace opfc {
 
 // ---------------------------------------------------------------------------
 // column pass: batched FFT along a strided axis (y or z), optional ETD update
@@ -332,6 +337,12 @@ __global__ void __launch_bounds__(Width<Real>::W *(M / Plan<M>::E)) x_kernel(con
   x_post_store<C, M, W, NT>(buf, tw, reinterpret_cast<C *>(a.out), a.nyq_off, row0, a.rows, tid);
 }
 
+}  // namespace opfc
+
+#include "x_tma.cuh"
+
+namespace opfc {
+
 // ---------------------------------------------------------------------------
 // small helper kernels (not on the per-step hot path except herm_fix)
 // ---------------------------------------------------------------------------
@@ -490,9 +501,63 @@ __global__ void energy_k_kernel(const typename Cx<Real>::T *ph, int M, int n1, i
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
+// Rebuild a segment's tiling for tile width W (strides do not depend on W).
+static inline ColSeg retile(ColSeg g, int W, int Wold) {
+  if (g.ntiles == 0) return g;
+  const int n_outer = g.ntiles / g.tiles_inner;
+  (void)Wold;
+  g.tiles_inner = (g.ncols + W - 1) / W;
+  g.ntiles = g.tiles_inner * n_outer;
+  return g;
+}
+
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
+static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
+  using C = typename Cx<Real>::T;
+  constexpr int W = tma_col_width(N, (int)sizeof(C), MODE);
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL>;
+  if constexpr (Cfg::STAGES < 1) {
+    return -1;
+  } else {
+    if (L.seg[0].ncols % W != 0 || L.seg[0].col_stride != 1) return -1;
+    constexpr int NT = W * (N / Plan<N>::E);
+    auto k = col_tma_kernel<Real, N, W, MODE, DIR, MODEL, INV>;
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+      attr = true;
+    }
+    ColArgs<Real> a;
+    a.seg0 = retile(L.seg[0], W, Width<Real>::W);
+    a.seg1 = L.nseg < 2 ? ColSeg{} : retile(L.seg[1], W, Width<Real>::W);
+    a.in[0] = L.in[0];
+    a.in[1] = L.in[1];
+    a.out[0] = L.out[0];
+    a.out[1] = L.out[1];
+    a.tw = L.tw;
+    a.psi_hat = L.psi_hat;
+    a.tab_a = reinterpret_cast<const Real *>(L.tab_a);
+    a.tab_b = reinterpret_cast<const Real *>(L.tab_b);
+    a.tab_chi = reinterpret_cast<const Real *>(L.tab_chi);
+    const CUtensorMap *t0 = reinterpret_cast<const CUtensorMap *>(L.tmap[0]);
+    auto pick = [&](int i) { return L.tmap[i] ? *reinterpret_cast<const CUtensorMap *>(L.tmap[i]) : *t0; };
+    int G = L.num_sms > 0 ? L.num_sms : 148;
+    const int most = a.seg0.ntiles > a.seg1.ntiles ? a.seg0.ntiles : a.seg1.ntiles;
+    if (G > most) G = most;
+    if (G < 1) return 0;
+    dim3 grid(G, MODE == COL_PLAIN ? L.nsets : 1);
+    k<<<grid, NT, Cfg::SMEM, s>>>(*t0, pick(1), pick(2), pick(3), pick(4), a, L.axis, L.flag);
+    return (int)cudaGetLastError();
+  }
+}
+
 template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
 static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
   using C = typename Cx<Real>::T;
+  if (L.tmap[0]) {
+    const int rc = launch_col_tma<Real, N, MODE, DIR, MODEL, INV>(L, s);
+    if (rc >= 0) return rc;
+  }
   constexpr int W = Width<Real>::W;
   constexpr int NT = W * (N / Plan<N>::E);
   const size_t smem = sizeof(C) * ((size_t)N + (size_t)N * (W + 1));
@@ -542,6 +607,47 @@ static int launch_col_n(const ColLaunch &L, cudaStream_t s) {
   return (int)cudaErrorInvalidValue;
 }
 
+template <typename Real, int M, int MODEL>
+static int launch_x_tma(const XLaunch &L, cudaStream_t s) {
+  if constexpr (M < 16) {
+    return -1;
+  } else {
+    using Cfg = XCfg<Real, M, MODEL>;
+    if (L.rows % Cfg::W != 0 || Cfg::SMEM > (size_t)kMaxDynSmem) return -1;
+    constexpr int NT = Cfg::W * (M / Plan<M>::E);
+    auto k = x_tma_kernel<Real, M, MODEL>;
+    static int occ = 0;
+    if (!occ) {
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, NT, Cfg::SMEM) != cudaSuccess || occ < 1)
+        occ = 1;
+    }
+    XArgs<Real> a;
+    a.in0 = L.in0;
+    a.in1 = L.in1;
+    a.out = L.out;
+    a.rin = nullptr;
+    a.rout = nullptr;
+    a.tw = L.tw;
+    a.nyq_off = L.nyq_off;
+    a.rows = L.rows;
+    a.scale = L.scale;
+    a.mean = L.mean;
+    a.c0 = (Real)L.c[0];
+    a.c1 = (Real)L.c[1];
+    a.c2 = (Real)L.c[2];
+    a.c3 = (Real)L.c[3];
+    a.c4 = (Real)L.c[4];
+    a.c5 = (Real)L.c[5];
+    a.flag = L.flag;
+    const int ntiles = L.rows / Cfg::W;
+    int G = (L.num_sms > 0 ? L.num_sms : 148) * occ;
+    if (G > ntiles) G = ntiles;
+    k<<<G, NT, Cfg::SMEM, s>>>(a);
+    return (int)cudaGetLastError();
+  }
+}
+
 template <typename Real, int M, int MODE, int MODEL>
 static int launch_x_t(const XLaunch &L, cudaStream_t s) {
   using C = typename Cx<Real>::T;
@@ -581,6 +687,15 @@ template <typename Real, int M>
 static int launch_x_m(const XLaunch &L, cudaStream_t s) {
   if (L.mode == X_R2C) return launch_x_t<Real, M, X_R2C, 0>(L, s);
   if (L.mode == X_C2R) return launch_x_t<Real, M, X_C2R, 0>(L, s);
+  if (L.use_tma) {
+    int rc = -1;
+    switch (L.model) {
+      case MK_PLAIN: rc = launch_x_tma<Real, M, MK_PLAIN>(L, s); break;
+      case MK_TUNGSTEN: rc = launch_x_tma<Real, M, MK_TUNGSTEN>(L, s); break;
+      case MK_FILTERED: rc = launch_x_tma<Real, M, MK_FILTERED>(L, s); break;
+    }
+    if (rc >= 0) return rc;
+  }
   switch (L.model) {
     case MK_PLAIN: return launch_x_t<Real, M, X_FUSED, MK_PLAIN>(L, s);
     case MK_TUNGSTEN: return launch_x_t<Real, M, X_FUSED, MK_TUNGSTEN>(L, s);

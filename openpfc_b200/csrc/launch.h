@@ -48,7 +48,25 @@ struct ColLaunch {
   const void *tab_a;  // opL / exp_Ldt
   const void *tab_b;  // opN / n_weight
   const void *tab_chi;  // mean-field filter (TUNGSTEN, FILTERED)
+  // TMA path (main segment): host CUtensorMap objects, see tma_col_width().
+  // PLAIN: tmap[0], tmap[1] = input of array set 0 / 1; UPDATE: A, psi_hat,
+  // tab_a, tab_b, tab_chi.  tmap[0] == nullptr selects the direct-load kernel.
+  const void *tmap[5];
+  int axis;            // 1 = y, 2 = z
+  unsigned int *flag;  // bit 1: a bounded wait expired
+  int num_sms;
 };
+
+// Tile width (columns) of the TMA column kernels: 128-byte rows for the plain
+// transforms and 64-byte rows for the fused update (which stages psi_hat and the
+// tables too), capped so one tile stays near 64 KB / 32 KB.  Host and device
+// use this one definition.
+constexpr int tma_col_width(int N, int csize, int mode) {
+  int w = (mode == COL_PLAIN ? 128 : 64) / csize;
+  const int cap = (mode == COL_PLAIN ? 65536 : 32768) / (N * csize);
+  if (cap < w) w = cap;
+  return w < 4 ? 4 : w;
+}
 
 enum XMode { X_R2C = 0, X_C2R = 1, X_FUSED = 2 };
 
@@ -67,7 +85,9 @@ struct XLaunch {
   double scale;      // C2R normalisation 1/(N0 N1 N2)
   double mean;       // mean density added after the C2R (k = 0 mode in FP64)
   double c[8];       // nonlinearity coefficients
-  unsigned int *flag;  // set to 1 when a non-finite value is produced
+  unsigned int *flag;  // bit 0: a non-finite value was produced; bit 1: a wait expired
+  int use_tma;         // X_FUSED: persistent bulk-copy-fed kernel when the size allows
+  int num_sms;
 };
 
 // Kernel launchers (kernels_f32.cu / kernels_f64.cu).  Return cudaError_t as int.

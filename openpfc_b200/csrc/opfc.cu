@@ -8,12 +8,14 @@
 // F[psi] -> multiply -> F^-1 -> nonlinearity -> F -> ETD combine -> F^-1
 // (apps/tungsten/include/tungsten/cpu/tungsten_model.hpp:306-366,
 //  docs/api/examples/10_complete_pfc_model.cpp:121-144).
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <random>
@@ -137,6 +139,15 @@ struct opfc_handle {
 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
+
+  bool use_tma = true;  // TMA-fed column passes (OPFC_NO_TMA=1 disables)
+  int num_sms = 148;
+  struct Tmap {
+    const void *ptr;
+    int axis, W, real;
+    CUtensorMap map;
+  };
+  std::vector<Tmap> tmaps;
   std::string err;
 };
 
@@ -244,12 +255,41 @@ void col_segments(const opfc_handle *h, int axis, ColLaunch &L) {
   L.N = (axis == 1) ? n1 : n2;
 }
 
-int col(opfc_handle *h, const ColLaunch &L) {
+int col(opfc_handle *h, ColLaunch L) {
+  L.flag = h->flag;
+  L.num_sms = h->num_sms;
   return h->prec == OPFC_FP64 ? launch_col<double>(L, h->stream) : launch_col<float>(L, h->stream);
 }
 int xpass(opfc_handle *h, const XLaunch &L) {
   return h->prec == OPFC_FP64 ? launch_x<double>(L, h->stream) : launch_x<float>(L, h->stream);
 }
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda link).
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                   const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                   const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      cudaGetLastError();
+  }
+  return fn;
+}
+
+// Tensor map of a split-layout array's main part viewed as scalars
+// [N2][N1][S*M] (S = 2 for complex, 1 for real tables), box = W columns x
+// min(N, 256) rows of `axis`.  Cached per (pointer, axis, W, real).
+const CUtensorMap *tmap_for(opfc_handle *h, const void *ptr, int axis, int W, bool real);
 
 // plain batched transform along y/z, in place (in == out) or out of place
 int col_plain(opfc_handle *h, int axis, int dir, const void *in0, void *out0,
@@ -264,7 +304,42 @@ int col_plain(opfc_handle *h, int axis, int dir, const void *in0, void *out0,
   L.in[1] = in1 ? in1 : in0;
   L.out[1] = out1 ? out1 : out0;
   L.tw = axis == 1 ? h->tw_y : h->tw_z;
+  L.axis = axis;
+  const int W = tma_col_width(L.N, 2 * (int)h->rsz, COL_PLAIN);
+  if (h->use_tma && L.N > 1 && h->M % W == 0) {
+    L.tmap[0] = tmap_for(h, in0, axis, W, false);
+    L.tmap[1] = in1 ? tmap_for(h, in1, axis, W, false) : nullptr;
+    if (in1 && !L.tmap[1]) L.tmap[0] = nullptr;
+  }
   return col(h, L);
+}
+
+const CUtensorMap *tmap_for(opfc_handle *h, const void *ptr, int axis, int W, bool real) {
+  if (!ptr) return nullptr;
+  for (const auto &t : h->tmaps)
+    if (t.ptr == ptr && t.axis == axis && t.W == W && t.real == (int)real) return &t.map;
+  EncodeTiledFn enc = encode_fn();
+  // returned pointers must stay valid while a launch is assembled: never grow
+  if (!enc || h->tmaps.size() == h->tmaps.capacity()) return nullptr;
+  const cuuint64_t es = h->rsz, S = real ? 1 : 2;
+  const int N = axis == 1 ? h->n1 : h->n2;
+  const cuuint32_t RB = (cuuint32_t)std::min(N, 256);
+  cuuint64_t dims[3] = {S * (cuuint64_t)h->M, (cuuint64_t)h->n1, (cuuint64_t)h->n2};
+  cuuint64_t strides[2] = {S * h->M * es, S * h->M * (cuuint64_t)h->n1 * es};
+  cuuint32_t box[3] = {(cuuint32_t)(S * W), axis == 1 ? RB : 1u, axis == 1 ? 1u : RB};
+  cuuint32_t estr[3] = {1, 1, 1};
+  opfc_handle::Tmap t{};
+  t.ptr = ptr;
+  t.axis = axis;
+  t.W = W;
+  t.real = (int)real;
+  const CUresult r = enc(&t.map, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         3, const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return nullptr;
+  h->tmaps.push_back(t);
+  return &h->tmaps.back().map;
 }
 
 XLaunch x_base(opfc_handle *h) {
@@ -276,6 +351,8 @@ XLaunch x_base(opfc_handle *h) {
   L.scale = 1.0 / ((double)h->n0 * h->n1 * h->n2);
   L.mean = 0.0;
   L.flag = h->flag;
+  L.use_tma = h->use_tma;
+  L.num_sms = h->num_sms;
   return L;
 }
 
@@ -375,6 +452,16 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.tab_a = h->tab_a;
     Z.tab_b = h->tab_b;
     Z.tab_chi = h->tab_chi;
+    Z.axis = 2;
+    const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE);
+    if (h->use_tma && Z.N > 1 && h->M % W == 0) {
+      Z.tmap[0] = tmap_for(h, h->work_a, 2, W, false);
+      Z.tmap[1] = tmap_for(h, h->psi_hat, 2, W, false);
+      Z.tmap[2] = tmap_for(h, h->tab_a, 2, W, true);
+      Z.tmap[3] = tmap_for(h, h->tab_b, 2, W, true);
+      Z.tmap[4] = h->tab_chi ? tmap_for(h, h->tab_chi, 2, W, true) : nullptr;
+      if (!Z.tmap[1] || !Z.tmap[2] || !Z.tmap[3] || (h->tab_chi && !Z.tmap[4])) Z.tmap[0] = nullptr;
+    }
     LAUNCH_TRY(h, col(h, Z));
   }
   if (only < 0 || only == 4) {  // Hermitian projection of the kx = 0 / Nyquist planes
@@ -674,6 +761,10 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   h->prec = d->precision;
   h->rsz = h->prec == OPFC_FP64 ? 8 : 4;
   h->device = d->device;
+  {
+    const char *no = std::getenv("OPFC_NO_TMA");
+    h->use_tma = !(no && no[0] == '1');
+  }
   cudaError_t e = cudaSetDevice(h->device);
   if (e != cudaSuccess) return OPFC_ERR_CUDA;
   if (d->stream) {
@@ -699,6 +790,9 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   if ((rc = dev_alloc(hp, (void **)&hp->partials, sizeof(double) * hp->npartials))) return cleanup(rc);
   if (cudaMemset(hp->flag, 0, sizeof(unsigned int)) != cudaSuccess) return cleanup(OPFC_ERR_CUDA);
   if (cudaMemset(hp->psi_hat, 0, cb) != cudaSuccess) return cleanup(OPFC_ERR_CUDA);
+  if (cudaDeviceGetAttribute(&hp->num_sms, cudaDevAttrMultiProcessorCount, hp->device) != cudaSuccess)
+    hp->num_sms = 148;
+  hp->tmaps.reserve(64);
   *out = h.release();
   return OPFC_OK;
 }
@@ -888,6 +982,7 @@ int opfc_sync(opfc_handle *h) {
   CUDA_TRY(h, cudaMemcpy(&f, h->flag, sizeof f, cudaMemcpyDeviceToHost));
   if (f) {
     cudaMemset(h->flag, 0, sizeof f);
+    if (f & 2u) return fail(h, OPFC_ERR_TIMEOUT, "a bounded device wait expired (TMA load never landed)");
     return fail(h, OPFC_ERR_NONFINITE, "non-finite value produced by the nonlinearity");
   }
   return OPFC_OK;

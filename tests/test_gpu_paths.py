@@ -1,0 +1,78 @@
+"""Both kernel families against the oracle: the persistent TMA/bulk-copy-fed
+passes (default) and the direct-load passes (OPFC_NO_TMA=1, read at handle
+creation), for every model and both precisions."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+import openpfc_b200 as ob
+
+pytestmark = pytest.mark.gpu
+
+PI4 = [math.pi / 4] * 3
+
+
+@pytest.fixture(params=["tma", "direct"])
+def path(request, monkeypatch):
+    if request.param == "direct":
+        monkeypatch.setenv("OPFC_NO_TMA", "1")
+    else:
+        monkeypatch.delenv("OPFC_NO_TMA", raising=False)
+    return request.param
+
+
+def rel_l2(a, b):
+    return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+
+@pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 256), (256, 16, 512)])
+def test_plain(oracle, path, prec, tol, n):
+    psi0 = oracle.ic_noise(n, -0.285, 0.01, 3)
+    ref = oracle.run_plain(psi0, PI4, -0.25, 0.5, 10)
+    m = ob.PfcB200(n, PI4, precision=prec)
+    m.initialize(0.5)
+    m.set_psi(psi0)
+    m.step(10)
+    m.sync()
+    assert rel_l2(m.get_psi(), ref) <= tol
+
+
+@pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
+def test_filtered(oracle, path, prec, tol):
+    n = (64, 64, 32)
+    psi0 = oracle.ic_seeds(n, PI4, -0.10, 0.001, 2, 8.0, 0.2, 4)
+    ref = oracle.run_filtered(psi0, PI4, -0.3, 0.5, -0.1, -0.5, 0.3, 0.5, 10)
+    m = ob.FilteredB200(n, PI4, precision=prec)
+    m.initialize(0.5)
+    m.set_psi(psi0)
+    m.step(10)
+    m.sync()
+    assert rel_l2(m.get_psi(), ref) <= tol
+
+
+@pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
+def test_tungsten(oracle, path, prec, tol):
+    n, dx = (64, 64, 64), 1.1107207345395915
+    psi0 = np.full((64, 64, 64), -0.4)
+    psi0 = oracle.ic_seed_inside(psi0, [dx] * 3, [-0.5 * dx * 64] * 3, 20.0, -0.047, 0.215936)
+    p = oracle.TungstenParams.defaults()
+    ref = oracle.run_tungsten(psi0, [dx] * 3, p, 1.0, 5)
+    m = ob.TungstenB200(n, [dx] * 3, precision=prec)
+    m.initialize(1.0)
+    m.set_psi(psi0)
+    m.step(5)
+    m.sync()
+    assert rel_l2(m.get_psi(), ref) <= tol
+
+
+def test_transforms(oracle, path):
+    n = (128, 64, 512)
+    x = np.random.default_rng(2).standard_normal((n[2], n[1], n[0]))
+    f = ob.B200Fft(n, precision=ob.FP64)
+    X = f.forward(x)
+    Xo = oracle.r2c(x)
+    assert np.abs(X - Xo).max() <= 1e-12 * np.abs(Xo).max()
+    assert np.abs(f.backward(Xo) - oracle.c2r(Xo, n[0])).max() <= 1e-12 * np.abs(x).max()
