@@ -162,6 +162,23 @@ int opfc_ic_seed(double *psi, const int n[3], const double dx[3], const double o
 int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, double noise,
                   int nseeds, double radius_cells, double amp, uint64_t seed);
 
+/* Forward R2C transform that allocates nothing (no counterpart in the
+ * reference; it is opfc_fft_forward without a handle).  For callers that cannot
+ * call cudaMalloc -- code inside CUDA graph capture, allocation-free real-time
+ * loops, hosts whose memory manager owns every device allocation.  in_real and
+ * out_complex are device pointers of the given precision (OPFC_FP32/OPFC_FP64)
+ * in the boundary layout above; the work is queued on `stream` (NULL = legacy
+ * default stream) and the call does not wait for it.
+ * The intermediate half spectrum lives in a fixed 16 MiB device array inside
+ * the library (held by every GPU that loads it until exit):
+ * (N0/2+1)*N1*N2 * (8 bytes FP32 | 16 bytes FP64) must be <= 16 MiB and every
+ * axis <= 1024, else OPFC_ERR_SIZE.  The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress) with the device current; make
+ * that first call before any stream capture.  All calls share the array and the
+ * twiddle tables next to it: calls that overlap on the GPU race. */
+int opfc_fft_forward_noalloc(const void *in_real, void *out_complex, const int n[3], int precision,
+                             void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,6 +105,7 @@ def lib():
     L.opfc_ic_noise.argtypes = [dp, sz, cd, cd, ctypes.c_uint64]
     L.opfc_ic_seed.argtypes = [dp, ip, dp, dp, dp, cd, cd, cd, ci]
     L.opfc_ic_seeds.argtypes = [dp, ip, dp, cd, cd, ci, cd, cd, ctypes.c_uint64]
+    L.opfc_fft_forward_noalloc.argtypes = [vp, vp, ip, ci, vp]
     _lib = L
     return L
 

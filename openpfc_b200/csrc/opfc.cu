@@ -25,6 +25,7 @@
 
 #include "../../include/openpfc_b200.h"
 #include "launch.h"
+#include "twiddle.h"
 
 using namespace opfc;
 
@@ -41,38 +42,7 @@ bool supported_len(int n) {
   return false;
 }
 
-// cos/sin(2 pi k / n) with octant reduction so that quarter turns are exact.
-void unit_root(long k, long n, double *c, double *s) {
-  k %= n;
-  if (k < 0) k += n;
-  if (n % 8 == 0) {
-    const long oct = (8 * k) / n;
-    const long rem = k - oct * (n / 8);
-    const double a = 2.0 * kPi * (double)rem / (double)n;
-    const double ca = std::cos(a), sa = std::sin(a);
-    const double r2 = 0.70710678118654752440084436210484903928;
-    double cc, ss;
-    switch (oct) {
-      case 0: cc = ca; ss = sa; break;
-      case 1: cc = r2 * (ca - sa); ss = r2 * (ca + sa); break;
-      case 2: cc = -sa; ss = ca; break;
-      case 3: cc = -r2 * (ca + sa); ss = r2 * (ca - sa); break;
-      case 4: cc = -ca; ss = -sa; break;
-      case 5: cc = -r2 * (ca - sa); ss = -r2 * (ca + sa); break;
-      case 6: cc = sa; ss = -ca; break;
-      default: cc = r2 * (ca + sa); ss = -r2 * (ca - sa); break;
-    }
-    *c = cc;
-    *s = ss;
-    return;
-  }
-  if (4 * k == n) { *c = 0; *s = 1; return; }
-  if (2 * k == n) { *c = -1; *s = 0; return; }
-  if (4 * k == 3 * n) { *c = 0; *s = -1; return; }
-  const double a = 2.0 * kPi * (double)k / (double)n;
-  *c = std::cos(a);
-  *s = std::sin(a);
-}
+void unit_root(long k, long n, double *c, double *s) { unit_root_host(k, n, c, s); }
 
 double neumaier(const double *a, size_t n) {
   double s = 0, c = 0;
