@@ -144,6 +144,20 @@ int opfc_profile_step(opfc_handle *h, int reps, double *ms, int max_kernels);
 /* Name of kernel k of the step ("y_inverse", "x_fused", ...). */
 const char *opfc_step_kernel_name(int k);
 
+/* Adjoint of the plain model (no counterpart in the reference, which has no
+ * differentiation).  opfc_set_r changes r (PLAIN/FILTERED) and rebuilds the
+ * tables.  opfc_forward_checkpointed advances n_steps from the current state,
+ * keeping a device snapshot of psi_hat every K steps.  opfc_adjoint then takes
+ * dLoss/dpsi_T (real field, count N0*N1*N2) and returns dLoss/dpsi_0 (same
+ * dtype/location), dLoss/dr and dLoss/dn0 = sum(dLoss/dpsi_0), re-running each
+ * K-step segment from its snapshot and stepping the adjoint
+ *   lambda_n = F^-1[opL F lambda] + 3 psi_n^2 F^-1[opN F lambda]
+ * backwards; the handle is left at the forward run's final state. */
+int opfc_set_r(opfc_handle *h, double r);
+int opfc_forward_checkpointed(opfc_handle *h, int n_steps, int K);
+int opfc_adjoint(opfc_handle *h, const void *grad_psi_T, int dtype, int where, void *grad_psi0,
+                 double *grad_r, double *grad_n0);
+
 /* Initial conditions, host-side (set-up only), x-fastest cell order.
  * Random numbers: one draw of std::mt19937_64(seed) per number, mapped to
  * [0,1) as (draw >> 11) * 2^-53.

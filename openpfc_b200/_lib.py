@@ -106,6 +106,9 @@ def lib():
     L.opfc_ic_seed.argtypes = [dp, ip, dp, dp, dp, cd, cd, cd, ci]
     L.opfc_ic_seeds.argtypes = [dp, ip, dp, cd, cd, ci, cd, cd, ctypes.c_uint64]
     L.opfc_fft_forward_noalloc.argtypes = [vp, vp, ip, ci, vp]
+    L.opfc_set_r.argtypes = [H, cd]
+    L.opfc_forward_checkpointed.argtypes = [H, ci, ci]
+    L.opfc_adjoint.argtypes = [H, vp, ci, ci, vp, dp, dp]
     _lib = L
     return L
 

@@ -22,7 +22,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libopenpfc_b200.so")
 SOURCES = ["kernels_f32.cu", "kernels_f64.cu", "opfc.cu", "noalloc.cu"]
-HEADERS = ["fft_core.cuh", "kernels.cuh", "launch.h", "col_tma.cuh", "x_tma.cuh", "twiddle.h"]
+HEADERS = ["fft_core.cuh", "kernels.cuh", "launch.h", "col_tma.cuh", "x_tma.cuh", "x_sq.cuh", "twiddle.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",

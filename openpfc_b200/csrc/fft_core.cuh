@@ -103,6 +103,41 @@ template <int DIR, typename C> struct Dft<8, DIR, C> {
   }
 };
 
+// 16 = 4 x 4: n = 4 n1 + n2, k = k1 + 4 k2 (DFT4 over n1, twiddle W16^{n2 k1},
+// DFT4 over n2, then a 4 x 4 transpose of the register order).
+template <int DIR, typename C> struct Dft<16, DIR, C> {
+  static __device__ __forceinline__ C w(C a, decltype(C::x) c, decltype(C::x) s) {
+    // a * (c + DIR i s)
+    return DIR < 0 ? mk<C>(a.x * c + a.y * s, a.y * c - a.x * s) : mk<C>(a.x * c - a.y * s, a.y * c + a.x * s);
+  }
+  static __device__ __forceinline__ void run(C (&v)[16]) {
+    using S = decltype(C::x);
+    const S c1 = S(0.92387953251128675612818318939678829);  // cos(pi/8)
+    const S s1 = S(0.38268343236508977172845998403039887);  // sin(pi/8)
+    const S h = S(0.70710678118654752440084436210484904);
+#pragma unroll
+    for (int n2 = 0; n2 < 4; ++n2) Dft<4, DIR, C>::run4(v[n2], v[n2 + 4], v[n2 + 8], v[n2 + 12]);
+    v[5] = w(v[5], c1, s1);    // W16^1
+    v[9] = w(v[9], h, h);      // W16^2
+    v[13] = w(v[13], s1, c1);  // W16^3
+    v[6] = w(v[6], h, h);      // W16^2
+    v[10] = rot90<DIR>(v[10]);  // W16^4
+    v[14] = w(v[14], -h, h);   // W16^6
+    v[7] = w(v[7], s1, c1);    // W16^3
+    v[11] = w(v[11], -h, h);   // W16^6
+    v[15] = w(v[15], -c1, -s1);  // W16^9
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) Dft<4, DIR, C>::run4(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    C t[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) t[i] = v[i];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+      for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[4 * k1 + k2];
+  }
+};
+
 template <int DIR, typename C> struct Dft<3, DIR, C> {
   static __device__ __forceinline__ void run(C (&v)[3]) {
     using S = decltype(C::x);

@@ -340,6 +340,7 @@ __global__ void __launch_bounds__(Width<Real>::W *(M / Plan<M>::E)) x_kernel(con
 }  // namespace opfc
 
 #include "x_tma.cuh"
+#include "x_sq.cuh"
 
 namespace opfc {
 
@@ -607,6 +608,47 @@ static int launch_col_n(const ColLaunch &L, cudaStream_t s) {
   return (int)cudaErrorInvalidValue;
 }
 
+template <typename Real> static XArgs<Real> x_args(const XLaunch &L) {
+  XArgs<Real> a;
+  a.in0 = L.in0;
+  a.in1 = L.in1;
+  a.out = L.out;
+  a.rin = reinterpret_cast<const Real *>(L.rin);
+  a.rout = reinterpret_cast<Real *>(L.rout);
+  a.tw = L.tw;
+  a.nyq_off = L.nyq_off;
+  a.rows = L.rows;
+  a.scale = L.scale;
+  a.mean = L.mean;
+  a.c0 = (Real)L.c[0];
+  a.c1 = (Real)L.c[1];
+  a.c2 = (Real)L.c[2];
+  a.c3 = (Real)L.c[3];
+  a.c4 = (Real)L.c[4];
+  a.c5 = (Real)L.c[5];
+  a.flag = L.flag;
+  return a;
+}
+
+template <typename Real, int R, int MODEL>
+static int launch_x_sq(const XLaunch &L, cudaStream_t s) {
+  using Cfg = XSqCfg<Real, R, MODEL>;
+  if (L.rows % Cfg::W != 0 || Cfg::SMEM > (size_t)kMaxDynSmem) return -1;
+  constexpr int NT = Cfg::W * R;
+  auto k = x_sq_kernel<Real, R, MODEL>;
+  static int occ = 0;
+  if (!occ) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, NT, Cfg::SMEM) != cudaSuccess || occ < 1)
+      occ = 1;
+  }
+  const int ntiles = L.rows / Cfg::W;
+  int G = (L.num_sms > 0 ? L.num_sms : 148) * occ;
+  if (G > ntiles) G = ntiles;
+  k<<<G, NT, Cfg::SMEM, s>>>(x_args<Real>(L));
+  return (int)cudaGetLastError();
+}
+
 template <typename Real, int M, int MODEL>
 static int launch_x_tma(const XLaunch &L, cudaStream_t s) {
   if constexpr (M < 16) {
@@ -689,6 +731,15 @@ static int launch_x_m(const XLaunch &L, cudaStream_t s) {
   if (L.mode == X_C2R) return launch_x_t<Real, M, X_C2R, 0>(L, s);
   if (L.use_tma) {
     int rc = -1;
+    if constexpr (M == 64 || M == 256) {
+      constexpr int R = M == 64 ? 8 : 16;
+      switch (L.model) {
+        case MK_PLAIN: rc = launch_x_sq<Real, R, MK_PLAIN>(L, s); break;
+        case MK_TUNGSTEN: rc = launch_x_sq<Real, R, MK_TUNGSTEN>(L, s); break;
+        case MK_FILTERED: rc = launch_x_sq<Real, R, MK_FILTERED>(L, s); break;
+      }
+      if (rc >= 0) return rc;
+    }
     switch (L.model) {
       case MK_PLAIN: rc = launch_x_tma<Real, M, MK_PLAIN>(L, s); break;
       case MK_TUNGSTEN: rc = launch_x_tma<Real, M, MK_TUNGSTEN>(L, s); break;

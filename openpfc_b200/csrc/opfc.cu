@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/openpfc_b200.h"
+#include "fft_core.cuh"
 #include "launch.h"
 #include "twiddle.h"
 
@@ -106,6 +107,15 @@ struct opfc_handle {
   bool have_state = false;
   bool a_valid = false;
   double dt = 0.0;
+
+  // adjoint of the plain model: state snapshots every K steps of the last
+  // checkpointed forward run, the r-derivatives of the tables, and work arrays
+  std::vector<void *> ckpt;  // psi_hat at steps 0, K, 2K, ... and the final state
+  int ckpt_K = 0, ckpt_steps = 0;
+  std::vector<void *> seg;   // psi_hat of each step of one recomputed segment
+  void *tab_ar = nullptr, *tab_br = nullptr;
+  void *adj_c[2] = {nullptr, nullptr};
+  void *adj_r[3] = {nullptr, nullptr, nullptr};
 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
@@ -305,7 +315,12 @@ const CUtensorMap *tmap_for(opfc_handle *h, const void *ptr, int axis, int W, bo
   t.real = (int)real;
   const CUresult r = enc(&t.map, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
                          3, const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_SWIZZLE_NONE,
+                         // full 128-byte rows may pull in the neighbouring tile's
+                         // row; narrower rows (the update's 64/32-byte rows) fetch
+                         // only what they use
+                         S * W * es >= 128 ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+                                           : CU_TENSOR_MAP_L2_PROMOTION_NONE,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return nullptr;
   h->tmaps.push_back(t);
@@ -702,6 +717,13 @@ int opfc_destroy(opfc_handle *h) {
   void *bufs[] = {h->psi_hat, h->work_a, h->work_b, h->tab_a, h->tab_b, h->tab_chi,
                   h->tw_x, h->tw_y, h->tw_z, h->real_buf, h->flag, h->partials};
   for (void *p : bufs)
+    if (p) cudaFree(p);
+  for (void *p : h->ckpt)
+    if (p) cudaFree(p);
+  for (void *p : h->seg)
+    if (p) cudaFree(p);
+  void *adj[] = {h->tab_ar, h->tab_br, h->adj_c[0], h->adj_c[1], h->adj_r[0], h->adj_r[1], h->adj_r[2]};
+  for (void *p : adj)
     if (p) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   cudaSetDevice(dev_prev);
@@ -1160,6 +1182,289 @@ int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, do
 
 const char *opfc_step_kernel_name(int k) {
   return (k >= 0 && k < kStepKernels) ? kStepKernelNames[k] : "";
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint of the plain conserved PFC step (checkpoint-and-recompute).
+//
+// In real space one step is psi' = A psi + B (psi^3) with A = F^-1 opL F and
+// B = F^-1 opN F (10_complete_pfc_model.cpp:121-144).  opL, opN are real and
+// even in k, so A and B are symmetric and the adjoint step is
+//   lambda_n = A lambda_{n+1} + 3 psi_n^2 (B lambda_{n+1}).
+// With opL = exp(L dt), L = -k^2 (r + (1-k^2)^2) and opN = dt (-k^2) phi(L dt),
+// phi(x) = (e^x - 1)/x, the parameter derivative is
+//   dLoss/dr = sum_n <lambda_{n+1}, F^-1[dopL/dr psi_hat_n + dopN/dr N_hat_n]>
+//            = sum_n (1/N) sum_k w_kx Re(conj(lambda_hat) (...)),
+// dopL/dr = -k^2 dt opL,  dopN/dr = dt^2 k^4 phi'(L dt),
+// accumulated in FP64.  psi_n comes from re-running the forward step (the same
+// CUDA graph) from the nearest snapshot.
+// ---------------------------------------------------------------------------
+
+template <typename Real>
+__global__ void cube_kernel(const Real *x, Real *y, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const Real v = x[i];
+    y[i] = v * v * v;
+  }
+}
+
+template <typename Real>
+__global__ void adj_combine_kernel(const Real *u, const Real *psi, const Real *w, Real *lam, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const Real p = psi[i];
+    lam[i] = u[i] + Real(3) * p * p * w[i];
+  }
+}
+
+// U = opL lam_hat (in place over lam_hat), V = opN lam_hat (over n_hat, after
+// it is read), and FP64 partial sums of w_kx Re(conj(lam_hat)(dA psi_hat + dB n_hat)).
+template <typename Real>
+__global__ void adj_modes_kernel(typename opfc::Cx<Real>::T *lam_hat, const typename opfc::Cx<Real>::T *psi_hat,
+                                 typename opfc::Cx<Real>::T *n_hat, const Real *ta, const Real *tb,
+                                 const Real *tar, const Real *tbr, int M, long long nyq_off,
+                                 double *partials) {
+  __shared__ double red[256];
+  const long long nc = nyq_off + nyq_off / M;
+  double s = 0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nc;
+       i += (long long)gridDim.x * blockDim.x) {
+    const auto l = lam_hat[i];
+    const auto p = psi_hat[i];
+    const auto q = n_hat[i];
+    const double ar = tar[i], br = tbr[i];
+    const double gx = ar * p.x + br * q.x, gy = ar * p.y + br * q.y;
+    const int kx = i < nyq_off ? (int)(i % M) : M;
+    const double wgt = (kx == 0 || kx == M) ? 1.0 : 2.0;
+    s += wgt * ((double)l.x * gx + (double)l.y * gy);
+    const Real a = ta[i], b = tb[i];
+    lam_hat[i].x = a * l.x;
+    lam_hat[i].y = a * l.y;
+    n_hat[i].x = b * l.x;
+    n_hat[i].y = b * l.y;
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int hh = blockDim.x / 2; hh > 0; hh >>= 1) {
+    if (threadIdx.x < hh) red[threadIdx.x] += red[threadIdx.x + hh];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
+}
+
+namespace {
+
+const int kEltBlocks = 148 * 8;
+
+// real `in` (device, compute precision) -> split-layout spectrum `out`
+int fwd_real(opfc_handle *h, const void *in, void *out) {
+  XLaunch X = x_base(h);
+  X.mode = X_R2C;
+  X.rin = in;
+  X.out = out;
+  LAUNCH_TRY(h, xpass(h, X));
+  LAUNCH_TRY(h, col_plain(h, 1, -1, out, out));
+  LAUNCH_TRY(h, col_plain(h, 2, -1, out, out));
+  return OPFC_OK;
+}
+
+// split-layout spectrum `spec` (destroyed) -> real `out`, scaled by 1/N, + mean
+int bwd_real(opfc_handle *h, void *spec, void *out, double mean) {
+  LAUNCH_TRY(h, col_plain(h, 2, +1, spec, spec));
+  LAUNCH_TRY(h, col_plain(h, 1, +1, spec, spec));
+  XLaunch X = x_base(h);
+  X.mode = X_C2R;
+  X.in0 = spec;
+  X.rout = out;
+  X.mean = mean;
+  LAUNCH_TRY(h, xpass(h, X));
+  return OPFC_OK;
+}
+
+// phi'(x) for phi(x) = (e^x - 1)/x, stable near 0
+double dphi(double x) {
+  if (std::fabs(x) < 1e-4) return 0.5 + x / 3.0 + x * x / 8.0 + x * x * x / 30.0;
+  return (x * std::exp(x) - std::expm1(x)) / (x * x);
+}
+
+int adjoint_tables(opfc_handle *h) {
+  const int n0 = h->n0, n1 = h->n1, n2 = h->n2, H = h->M + 1;
+  const double f0 = 2.0 * kPi / (h->desc.dx[0] * n0);
+  const double f1 = 2.0 * kPi / (h->desc.dx[1] * n1);
+  const double f2 = 2.0 * kPi / (h->desc.dx[2] * n2);
+  const double r = h->desc.r, dt = h->dt;
+  std::vector<double> ar(h->nc), br(h->nc);
+  auto kc = [](int i, int n, double f) { return (i <= n / 2) ? i * f : (i - n) * f; };
+  parallel_for((long)n2 * n1, [&](long row) {
+    const int ky = (int)(row % n1), kz = (int)(row / n1);
+    for (int kx = 0; kx < H; ++kx) {
+      const double a = kc(kx, n0, f0), b = kc(ky, n1, f1), c = kc(kz, n2, f2);
+      const double k2 = a * a + b * b + c * c;
+      const double L = -k2 * (r + (1.0 - k2) * (1.0 - k2));
+      const size_t o = split_index(h, kx, ky, kz);
+      ar[o] = -k2 * dt * std::exp(L * dt);
+      br[o] = dt * dt * k2 * k2 * dphi(L * dt);
+    }
+  });
+  for (int t = 0; t < 2; ++t) {
+    void **dst = t == 0 ? &h->tab_ar : &h->tab_br;
+    std::vector<double> &src = t == 0 ? ar : br;
+    if (!*dst) {
+      int rc = dev_alloc(h, dst, h->nc * h->rsz);
+      if (rc) return rc;
+    }
+    if (h->prec == OPFC_FP64) {
+      CUDA_TRY(h, cudaMemcpy(*dst, src.data(), h->nc * 8, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(src.begin(), src.end());
+      CUDA_TRY(h, cudaMemcpy(*dst, f.data(), h->nc * 4, cudaMemcpyHostToDevice));
+    }
+  }
+  return OPFC_OK;
+}
+
+int copy_state(opfc_handle *h, void *dst, const void *src) {
+  CUDA_TRY(h, cudaMemcpyAsync(dst, src, h->nc * 2 * h->rsz, cudaMemcpyDeviceToDevice, h->stream));
+  return OPFC_OK;
+}
+
+int adjoint_buffers(opfc_handle *h) {
+  int rc;
+  for (auto &p : h->adj_c)
+    if (!p && (rc = dev_alloc(h, &p, h->nc * 2 * h->rsz))) return rc;
+  for (auto &p : h->adj_r)
+    if (!p && (rc = dev_alloc(h, &p, h->nr * h->rsz))) return rc;
+  while ((int)h->seg.size() < h->ckpt_K) {
+    void *p = nullptr;
+    if ((rc = dev_alloc(h, &p, h->nc * 2 * h->rsz))) return rc;
+    h->seg.push_back(p);
+  }
+  return OPFC_OK;
+}
+
+// lambda (adj_r[0]) <- adjoint of the step taken from psi_hat_n; adds the step's
+// dLoss/dr contribution to *dr.
+int adjoint_step(opfc_handle *h, const void *psi_hat_n, double *dr) {
+  void *lam = h->adj_r[0], *psi = h->adj_r[1], *tmp = h->adj_r[2];
+  void *c0 = h->adj_c[0], *c1 = h->adj_c[1];
+  const bool f64 = h->prec == OPFC_FP64;
+  int rc;
+  // psi_n in real space, N_hat_n = F[psi_n^3]
+  if ((rc = copy_state(h, c0, psi_hat_n))) return rc;
+  if ((rc = bwd_real(h, c0, psi, mean_density(h)))) return rc;
+  if (f64)
+    cube_kernel<double><<<kEltBlocks, 256, 0, h->stream>>>((const double *)psi, (double *)tmp, h->nr);
+  else
+    cube_kernel<float><<<kEltBlocks, 256, 0, h->stream>>>((const float *)psi, (float *)tmp, h->nr);
+  CUDA_TRY(h, cudaGetLastError());
+  if ((rc = fwd_real(h, tmp, c1))) return rc;
+  // lambda_hat = F[lambda_{n+1}]
+  if ((rc = fwd_real(h, lam, c0))) return rc;
+  if (f64)
+    adj_modes_kernel<double><<<h->npartials, 256, 0, h->stream>>>(
+        (double2 *)c0, (const double2 *)psi_hat_n, (double2 *)c1, (const double *)h->tab_a,
+        (const double *)h->tab_b, (const double *)h->tab_ar, (const double *)h->tab_br, h->M, h->nyq_off,
+        h->partials);
+  else
+    adj_modes_kernel<float><<<h->npartials, 256, 0, h->stream>>>(
+        (float2 *)c0, (const float2 *)psi_hat_n, (float2 *)c1, (const float *)h->tab_a,
+        (const float *)h->tab_b, (const float *)h->tab_ar, (const float *)h->tab_br, h->M, h->nyq_off,
+        h->partials);
+  CUDA_TRY(h, cudaGetLastError());
+  std::vector<double> part(h->npartials);
+  CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->partials, sizeof(double) * h->npartials,
+                              cudaMemcpyDeviceToHost, h->stream));
+  // u = F^-1[opL lambda_hat] -> lam ; w = F^-1[opN lambda_hat] -> tmp
+  if ((rc = bwd_real(h, c0, lam, 0.0))) return rc;
+  if ((rc = bwd_real(h, c1, tmp, 0.0))) return rc;
+  if (f64)
+    adj_combine_kernel<double><<<kEltBlocks, 256, 0, h->stream>>>(
+        (const double *)lam, (const double *)psi, (const double *)tmp, (double *)lam, h->nr);
+  else
+    adj_combine_kernel<float><<<kEltBlocks, 256, 0, h->stream>>>(
+        (const float *)lam, (const float *)psi, (const float *)tmp, (float *)lam, h->nr);
+  CUDA_TRY(h, cudaGetLastError());
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  *dr += neumaier(part.data(), part.size()) / (double)h->nr;
+  return OPFC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int opfc_set_r(opfc_handle *h, double r) {
+  if (!h) return OPFC_ERR_ARG;
+  if (h->desc.model == OPFC_MODEL_TUNGSTEN) return fail(h, OPFC_ERR_ARG, "r is not a Tungsten parameter");
+  h->desc.r = r;
+  release_graph(h);
+  h->ckpt_steps = 0;
+  if (h->initialized) return opfc_initialize(h, h->dt);
+  return OPFC_OK;
+}
+
+int opfc_forward_checkpointed(opfc_handle *h, int n_steps, int K) {
+  if (!h) return OPFC_ERR_ARG;
+  if (h->desc.model != OPFC_MODEL_PLAIN)
+    return fail(h, OPFC_ERR_ARG, "the adjoint is implemented for the plain PFC model");
+  if (n_steps < 1 || K < 1) return fail(h, OPFC_ERR_ARG, "need n_steps >= 1 and K >= 1");
+  if (!h->initialized || !h->have_state) return fail(h, OPFC_ERR_STATE, "need tables and a state");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  const int nck = (n_steps + K - 1) / K + 1;  // segment starts + final state
+  int rc;
+  while ((int)h->ckpt.size() < nck) {
+    void *p = nullptr;
+    if ((rc = dev_alloc(h, &p, h->nc * 2 * h->rsz))) return rc;
+    h->ckpt.push_back(p);
+  }
+  for (int s = 0; s < n_steps; ++s) {
+    if (s % K == 0 && (rc = copy_state(h, h->ckpt[s / K], h->psi_hat))) return rc;
+    if ((rc = opfc_step(h, 1))) return rc;
+  }
+  if ((rc = copy_state(h, h->ckpt[nck - 1], h->psi_hat))) return rc;
+  h->ckpt_K = K;
+  h->ckpt_steps = n_steps;
+  return opfc_sync(h);
+}
+
+int opfc_adjoint(opfc_handle *h, const void *grad_psi_T, int dtype, int where, void *grad_psi0,
+                 double *grad_r, double *grad_n0) {
+  if (!h || !grad_psi_T || !grad_psi0 || !grad_r || !grad_n0)
+    return h ? fail(h, OPFC_ERR_ARG, "null pointer") : OPFC_ERR_ARG;
+  int rc;
+  if ((rc = check_dtype_where(h, dtype, where))) return rc;
+  if (h->ckpt_steps < 1) return fail(h, OPFC_ERR_STATE, "run opfc_forward_checkpointed first");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  if ((rc = adjoint_tables(h))) return rc;  // r or dt may have changed since the last call
+  if ((rc = adjoint_buffers(h))) return rc;
+  // lambda_T = dLoss/dpsi_T
+  if ((rc = real_in(h, grad_psi_T, dtype, where))) return rc;
+  CUDA_TRY(h, cudaMemcpyAsync(h->adj_r[0], h->real_buf, h->nr * h->rsz, cudaMemcpyDeviceToDevice, h->stream));
+  const int K = h->ckpt_K, n = h->ckpt_steps;
+  const int nseg = (n + K - 1) / K;
+  double dr = 0.0;
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int len = std::min(K, n - sg * K);
+    // recompute the segment's states with the forward step itself
+    if ((rc = copy_state(h, h->psi_hat, h->ckpt[sg]))) return rc;
+    h->a_valid = false;
+    for (int i = 0; i < len; ++i) {
+      if ((rc = copy_state(h, h->seg[i], h->psi_hat))) return rc;
+      if ((rc = opfc_step(h, 1))) return rc;
+    }
+    for (int i = len - 1; i >= 0; --i)
+      if ((rc = adjoint_step(h, h->seg[i], &dr))) return rc;
+  }
+  // leave the handle at the end state of the forward run
+  if ((rc = copy_state(h, h->psi_hat, h->ckpt[nseg]))) return rc;
+  h->a_valid = false;
+  CUDA_TRY(h, cudaMemcpyAsync(h->real_buf, h->adj_r[0], h->nr * h->rsz, cudaMemcpyDeviceToDevice, h->stream));
+  if ((rc = device_sum(h, 1, grad_n0))) return rc;  // psi0 = n0 + noise: dLoss/dn0 = sum lambda_0
+  *grad_r = dr;
+  if ((rc = real_out(h, grad_psi0, dtype, where))) return rc;
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  return opfc_sync(h);
 }
 
 }  // extern "C"

@@ -1,0 +1,192 @@
+// x_sq.cuh -- fused x pass for half lengths M = R*R (R = 8, 16): one x-row is
+// owned by R lanes of one warp.
+//
+// The complex FFT of length M is a two-stage Stockham (radix R, then radix R
+// with twiddles W_M^{j r}); its single exchange is a padded R x (R+1) transpose
+// private to the warp (__syncwarp only).  Stage-2 twiddles come from a per-stage
+// table indexed [r-1][j], so the R lanes of a line read consecutive entries.
+// The C2R pre-processing reads the bulk-copied rows directly; the R2C
+// post-processing pairs Z[k] with Z[M-k] through warp shuffles (lane j holds
+// k = j + R m, its partner is lane R-j), and stores the modes straight to HBM.
+// Tiles of W rows arrive by cp.async.bulk exactly as in x_tma.cuh.
+#pragma once
+#include "x_tma.cuh"
+
+namespace opfc {
+
+template <typename Real, int R, int MODEL> struct XSqCfg {
+  using C = typename Cx<Real>::T;
+  static constexpr int M = R * R;
+  static constexpr int W = Width<Real>::W;  // rows (lines) per tile
+  static constexpr int P = M + 2;           // padded row pitch of the landed tile
+  static constexpr int EXL = R * (R + 1);   // exchange space per line
+  static constexpr size_t TILE = (size_t(W) * P + W) * sizeof(C);
+  static constexpr size_t EXCH = size_t(W) * EXL * sizeof(C);
+  static constexpr size_t BUF = align128(TILE > EXCH ? TILE : EXCH);
+  static constexpr int NARR = MODEL == MK_TUNGSTEN ? 2 : 1;
+  static constexpr size_t STAGE = BUF * NARR;
+  static constexpr size_t TW = align128(size_t(2 * M) * sizeof(C));
+  static constexpr size_t TWS = align128(size_t(R) * R * sizeof(C));
+  static constexpr int STAGES = 2;
+  static constexpr size_t SMEM = TW + TWS + STAGES * STAGE + 64;
+  static constexpr unsigned TX = unsigned((size_t(W) * M + W) * sizeof(C)) * NARR;
+};
+
+template <typename C> __device__ __forceinline__ C shfl_c(C v, int lane) {
+  C r;
+  r.x = __shfl_sync(0xffffffffu, v.x, lane);
+  r.y = __shfl_sync(0xffffffffu, v.y, lane);
+  return r;
+}
+
+// Length R*R transform of one line held as v[m] = x[j + R m]; same layout on exit.
+template <typename C, int R, int DIR>
+__device__ __forceinline__ void fft_sq(C (&v)[R], C *ex, int j, const C *tws) {
+  Dft<R, DIR, C>::run(v);  // stage 1 (Ns = 1): outputs y[j R + r]
+#pragma unroll
+  for (int r = 0; r < R; ++r) ex[j * (R + 1) + r] = v[r];
+  __syncwarp();
+#pragma unroll
+  for (int m = 0; m < R; ++m) v[m] = ex[m * (R + 1) + j];  // x[j + R m]
+  __syncwarp();
+#pragma unroll
+  for (int r = 1; r < R; ++r) v[r] = twmul<DIR>(v[r], tws[(r - 1) * R + j]);
+  Dft<R, DIR, C>::run(v);  // stage 2 (Ns = R): outputs x[j + R r]
+}
+
+template <typename Real, int R, int MODEL>
+__global__ void __launch_bounds__(Width<Real>::W *R) x_sq_kernel(const XArgs<Real> a) {
+  using Cfg = XSqCfg<Real, R, MODEL>;
+  using C = typename Cx<Real>::T;
+  constexpr int M = Cfg::M;
+  constexpr int W = Cfg::W;
+  constexpr int NT = W * R;
+  constexpr int N0 = 2 * M;
+  constexpr int STAGES = Cfg::STAGES;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *tws = reinterpret_cast<C *>(smraw + Cfg::TW);
+  unsigned char *stage0 = smraw + Cfg::TW + Cfg::TWS;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(stage0 + STAGES * Cfg::STAGE);
+
+  const int tid = threadIdx.x;
+  const int j = tid % R;
+  const int c = tid / R;
+  const int lane = tid & 31;
+  const int partner = (lane & ~(R - 1)) | ((R - j) & (R - 1));
+  const C *gtw = reinterpret_cast<const C *>(a.tw);
+  for (int i = tid; i < N0; i += NT) tw[i] = gtw[i];
+  for (int i = tid; i < (R - 1) * R; i += NT) {
+    const int r = i / R + 1, k = i % R;
+    tws[i] = gtw[(2 * k * r) % N0];  // W_M^{k r} = exp(-2 pi i k r / M)
+  }
+  if (tid == 0) {
+    for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  const int ntiles = a.rows / W;
+  const int G = gridDim.x;
+  const C *src[2] = {reinterpret_cast<const C *>(a.in0), reinterpret_cast<const C *>(a.in1)};
+  auto issue = [&](int s, int t) {
+    unsigned char *st = stage0 + s * Cfg::STAGE;
+    mbar_expect_tx(&bars[s], Cfg::TX);
+    const long long row0 = (long long)t * W;
+#pragma unroll
+    for (int q = 0; q < Cfg::NARR; ++q) {
+      C *tile = reinterpret_cast<C *>(st + q * Cfg::BUF);
+      for (int cc = 0; cc < W; ++cc)
+        bulk_load(tile + cc * Cfg::P, src[q] + (row0 + cc) * M, unsigned(M * sizeof(C)), &bars[s]);
+      bulk_load(tile + W * Cfg::P, src[q] + a.nyq_off + row0, unsigned(W * sizeof(C)), &bars[s]);
+    }
+  };
+  if (tid == 0)
+    for (int s = 0; s < STAGES; ++s) {
+      const int t = blockIdx.x + s * G;
+      if (t < ntiles) issue(s, t);
+    }
+
+  const Real sc = (Real)a.scale, mn = (Real)a.mean;
+  C *out = reinterpret_cast<C *>(a.out);
+  int it = 0;
+  bool alive = true, bad = false;
+  for (int t = blockIdx.x; t < ntiles; t += G, ++it) {
+    const int s = it % STAGES;
+    const bool ok = mbar_wait(&bars[s], (unsigned)(it / STAGES) & 1u);
+    if (!__syncthreads_and(ok)) {
+      alive = false;
+      break;
+    }
+    unsigned char *st = stage0 + s * Cfg::STAGE;
+    C *buf0 = reinterpret_cast<C *>(st);
+    C v[R];
+    x_pre_rows<C, M, Cfg::P, R>(buf0, buf0 + W * Cfg::P, tw, c, j, v);
+    if constexpr (MODEL == MK_TUNGSTEN) {
+      C *buf1 = reinterpret_cast<C *>(st + Cfg::BUF);
+      C u[R];
+      x_pre_rows<C, M, Cfg::P, R>(buf1, buf1 + W * Cfg::P, tw, c, j, u);
+      __syncthreads();  // landed rows consumed: the buffers become exchange space
+      fft_sq<C, R, +1>(v, buf0 + c * Cfg::EXL, j, tws);
+      fft_sq<C, R, +1>(u, buf1 + c * Cfg::EXL, j, tws);
+      // N = p3b u^2 + p4b u^3 + q3b v^2 + q4b v^3 - stabP u with u = psi, v = psi_MF
+      // (apps/tungsten/include/tungsten/cpu/tungsten_model.hpp:334-350)
+#pragma unroll
+      for (int m = 0; m < R; ++m) {
+        const Real ux = v[m].x * sc + mn, uy = v[m].y * sc + mn;
+        const Real vx = u[m].x * sc + mn, vy = u[m].y * sc + mn;
+        const Real nx = ux * ux * (a.c0 + a.c1 * ux) + vx * vx * (a.c2 + a.c3 * vx) - a.c4 * ux;
+        const Real ny = uy * uy * (a.c0 + a.c1 * uy) + vy * vy * (a.c2 + a.c3 * vy) - a.c4 * uy;
+        bad |= !(isfinite(nx) && isfinite(ny));
+        v[m] = mk<C>(nx, ny);
+      }
+    } else {
+      __syncthreads();
+      fft_sq<C, R, +1>(v, buf0 + c * Cfg::EXL, j, tws);
+#pragma unroll
+      for (int m = 0; m < R; ++m) {
+        const Real x = v[m].x * sc + mn, y = v[m].y * sc + mn;
+        Real nx, ny;
+        if constexpr (MODEL == MK_FILTERED) {
+          nx = x * x * (a.c0 + a.c1 * x + a.c2 * x * x);
+          ny = y * y * (a.c0 + a.c1 * y + a.c2 * y * y);
+        } else {
+          nx = x * x * x;
+          ny = y * y * y;
+        }
+        bad |= !(isfinite(nx) && isfinite(ny));
+        v[m] = mk<C>(nx, ny);
+      }
+    }
+    fft_sq<C, R, -1>(v, buf0 + c * Cfg::EXL, j, tws);
+    // R2C post-processing: X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W_N0^k (Z[k] - conj Z[M-k])
+    const long long row = (long long)t * W + c;
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      const int k = j + R * m;
+      C Y = shfl_c(v[R - 1 - m], partner);
+      if (j == 0) Y = v[(R - m) % R];
+      const C Z = v[m];
+      const C sm = mk<C>(Z.x + Y.x, Z.y - Y.y);
+      const C d = mk<C>(Z.x - Y.x, Z.y + Y.y);
+      const C e = twmul<-1>(d, tw[k]);
+      out[row * M + k] = mk<C>(Real(0.5) * (sm.x + e.y), Real(0.5) * (sm.y - e.x));
+    }
+    if (j == 0) out[a.nyq_off + row] = mk<C>(v[0].x - v[0].y, Real(0));
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      const int tn = t + STAGES * G;
+      if (tn < ntiles) issue(s, tn);
+    }
+  }
+  if (bad && a.flag) atomicOr(a.flag, 1u);
+  if (!alive) {
+    if (tid == 0 && a.flag) atomicOr(a.flag, 2u);
+    const int mine = (ntiles - (int)blockIdx.x + G - 1) / G;
+    const int issued = mine < it + STAGES ? mine : it + STAGES;
+    for (int k = it; k < issued; ++k) mbar_wait(&bars[k % STAGES], (unsigned)(k / STAGES) & 1u);
+  }
+}
+
+}  // namespace opfc

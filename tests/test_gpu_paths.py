@@ -28,7 +28,7 @@ def rel_l2(a, b):
 
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
-@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 256), (256, 16, 512)])
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 256), (256, 16, 512), (512, 32, 16)])
 def test_plain(oracle, path, prec, tol, n):
     psi0 = oracle.ic_noise(n, -0.285, 0.01, 3)
     ref = oracle.run_plain(psi0, PI4, -0.25, 0.5, 10)
@@ -41,8 +41,8 @@ def test_plain(oracle, path, prec, tol, n):
 
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
-def test_filtered(oracle, path, prec, tol):
-    n = (64, 64, 32)
+@pytest.mark.parametrize("n", [(64, 64, 32), (512, 16, 16), (128, 32, 32)])
+def test_filtered(oracle, path, prec, tol, n):
     psi0 = oracle.ic_seeds(n, PI4, -0.10, 0.001, 2, 8.0, 0.2, 4)
     ref = oracle.run_filtered(psi0, PI4, -0.3, 0.5, -0.1, -0.5, 0.3, 0.5, 10)
     m = ob.FilteredB200(n, PI4, precision=prec)
@@ -54,10 +54,12 @@ def test_filtered(oracle, path, prec, tol):
 
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
-def test_tungsten(oracle, path, prec, tol):
-    n, dx = (64, 64, 64), 1.1107207345395915
-    psi0 = np.full((64, 64, 64), -0.4)
-    psi0 = oracle.ic_seed_inside(psi0, [dx] * 3, [-0.5 * dx * 64] * 3, 20.0, -0.047, 0.215936)
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 64, 32), (512, 16, 32)])
+def test_tungsten(oracle, path, prec, tol, n):
+    dx = 1.1107207345395915
+    psi0 = np.full((n[2], n[1], n[0]), -0.4)
+    origin = [-0.5 * dx * n[a] for a in range(3)]
+    psi0 = oracle.ic_seed_inside(psi0, [dx] * 3, origin, 20.0, -0.047, 0.215936)
     p = oracle.TungstenParams.defaults()
     ref = oracle.run_tungsten(psi0, [dx] * 3, p, 1.0, 5)
     m = ob.TungstenB200(n, [dx] * 3, precision=prec)
