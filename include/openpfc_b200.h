@@ -153,6 +153,28 @@ const char *opfc_step_kernel_name(int k);
  * K-step segment from its snapshot and stepping the adjoint
  *   lambda_n = F^-1[opL F lambda] + 3 psi_n^2 F^-1[opN F lambda]
  * backwards; the handle is left at the forward run's final state. */
+/* Uneven-size ensembles (no counterpart in the reference, which runs one field
+ * per MPI job): `count` independent plain-PFC fields, each with its own size
+ * (N0/2 in {16,24,32,40,48,64}, N1, N2 in {16,32,48,64,80,96,128}), dx and r,
+ * one precision.  Every stage of a step is one persistent kernel over all
+ * members; opfc_ensemble_step(n) captures the n-step loop as one CUDA graph.
+ * Fields are host FP64 arrays (x fastest).  opfc_ensemble_autotune times the
+ * tile-shape variants of the column and x stages, caches the fastest (see
+ * OPENPFC_GPU_AUTOTUNE_* in the library notes) and invalidates the states. */
+typedef struct opfc_ensemble opfc_ensemble;
+int opfc_ensemble_create(int count, const opfc_desc *descs, opfc_ensemble **out);
+int opfc_ensemble_destroy(opfc_ensemble *e);
+const char *opfc_ensemble_last_error(const opfc_ensemble *e);
+int opfc_ensemble_initialize(opfc_ensemble *e, double dt);
+int opfc_ensemble_set_psi(opfc_ensemble *e, int member, const double *psi, size_t count);
+int opfc_ensemble_get_psi(opfc_ensemble *e, int member, double *psi, size_t count);
+int opfc_ensemble_step(opfc_ensemble *e, int n_steps);
+int opfc_ensemble_sync(opfc_ensemble *e);
+int opfc_ensemble_autotune(opfc_ensemble *e, double *ms_col, double *ms_x);
+int opfc_ensemble_variants(const opfc_ensemble *e, int *var_col, int *var_x);
+size_t opfc_ensemble_cells(const opfc_ensemble *e);
+void *opfc_ensemble_stream(const opfc_ensemble *e);
+
 int opfc_set_r(opfc_handle *h, double r);
 int opfc_forward_checkpointed(opfc_handle *h, int n_steps, int K);
 int opfc_adjoint(opfc_handle *h, const void *grad_psi_T, int dtype, int where, void *grad_psi0,

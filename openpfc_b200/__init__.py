@@ -325,3 +325,85 @@ def ic_seeds(n, dx, n0, noise, nseeds, radius_cells, amp, seed) -> np.ndarray:
     _check(None, lib().opfc_ic_seeds(_dp(psi), _i3(n), _d3(dx), n0, noise, nseeds, radius_cells,
                                      amp, seed))
     return psi
+
+
+# ---------------------------------------------------------------------------
+# uneven-size ensembles (opfc_ensemble_*)
+# ---------------------------------------------------------------------------
+
+class Ensemble:
+    """Independent plain-PFC fields of different sizes and parameters advanced
+    together: one persistent kernel per stage, the step loop in one CUDA graph.
+
+    members: sequence of dicts with keys n (N0, N1, N2), dx (3 values), r."""
+
+    def __init__(self, members, precision: int = FP32, device: int = 0):
+        descs = (Desc * len(members))()
+        for i, mb in enumerate(members):
+            lib().opfc_desc_default(ctypes.byref(descs[i]))
+            _geom(descs[i], mb["n"], mb["dx"], None, precision, device, None)
+            descs[i].model = MODEL_PLAIN
+            descs[i].r = float(mb["r"])
+        self._h = ctypes.c_void_p()
+        rc = lib().opfc_ensemble_create(len(members), descs, ctypes.byref(self._h))
+        if rc != 0:
+            if rc == -2:
+                raise ValueError("OPFC_ERR_SIZE: unsupported member size")
+            raise OpfcError(rc, "opfc_ensemble_create")
+        self.members = [dict(m) for m in members]
+        self.shapes = [(m["n"][2], m["n"][1], m["n"][0]) for m in members]
+
+    def _check(self, rc):
+        if rc != 0:
+            msg = lib().opfc_ensemble_last_error(self._h).decode()
+            if rc == -2:
+                raise ValueError(f"OPFC_ERR_SIZE: {msg}")
+            raise OpfcError(rc, msg)
+
+    def close(self):
+        if getattr(self, "_h", None) and self._h.value:
+            lib().opfc_ensemble_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def initialize(self, dt: float):
+        self._check(lib().opfc_ensemble_initialize(self._h, float(dt)))
+
+    def set_psi(self, i: int, psi: np.ndarray):
+        psi = np.ascontiguousarray(psi, dtype=np.float64)
+        self._check(lib().opfc_ensemble_set_psi(self._h, int(i), _dp(psi), psi.size))
+
+    def get_psi(self, i: int) -> np.ndarray:
+        out = np.empty(self.shapes[i], dtype=np.float64)
+        self._check(lib().opfc_ensemble_get_psi(self._h, int(i), _dp(out), out.size))
+        return out
+
+    def step(self, n_steps: int):
+        self._check(lib().opfc_ensemble_step(self._h, int(n_steps)))
+
+    def sync(self):
+        self._check(lib().opfc_ensemble_sync(self._h))
+
+    def autotune(self):
+        """Time the tile-shape variants, keep the fastest; states must be set again."""
+        mc, mx = (ctypes.c_double * 6)(), (ctypes.c_double * 6)()
+        self._check(lib().opfc_ensemble_autotune(self._h, mc, mx))
+        return list(mc), list(mx)
+
+    def variants(self):
+        a, b = ctypes.c_int(), ctypes.c_int()
+        self._check(lib().opfc_ensemble_variants(self._h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    @property
+    def cells(self) -> int:
+        return int(lib().opfc_ensemble_cells(self._h))
+
+    @property
+    def stream(self) -> int:
+        return int(lib().opfc_ensemble_stream(self._h) or 0)

@@ -106,6 +106,21 @@ def lib():
     L.opfc_ic_seed.argtypes = [dp, ip, dp, dp, dp, cd, cd, cd, ci]
     L.opfc_ic_seeds.argtypes = [dp, ip, dp, cd, cd, ci, cd, cd, ctypes.c_uint64]
     L.opfc_fft_forward_noalloc.argtypes = [vp, vp, ip, ci, vp]
+    L.opfc_ensemble_create.argtypes = [ci, ctypes.POINTER(Desc), ctypes.POINTER(H)]
+    L.opfc_ensemble_destroy.argtypes = [H]
+    L.opfc_ensemble_last_error.argtypes = [H]
+    L.opfc_ensemble_last_error.restype = ctypes.c_char_p
+    L.opfc_ensemble_initialize.argtypes = [H, cd]
+    L.opfc_ensemble_set_psi.argtypes = [H, ci, dp, sz]
+    L.opfc_ensemble_get_psi.argtypes = [H, ci, dp, sz]
+    L.opfc_ensemble_step.argtypes = [H, ci]
+    L.opfc_ensemble_sync.argtypes = [H]
+    L.opfc_ensemble_autotune.argtypes = [H, dp, dp]
+    L.opfc_ensemble_variants.argtypes = [H, ip, ip]
+    L.opfc_ensemble_cells.argtypes = [H]
+    L.opfc_ensemble_cells.restype = sz
+    L.opfc_ensemble_stream.argtypes = [H]
+    L.opfc_ensemble_stream.restype = vp
     L.opfc_set_r.argtypes = [H, cd]
     L.opfc_forward_checkpointed.argtypes = [H, ci, ci]
     L.opfc_adjoint.argtypes = [H, vp, ci, ci, vp, dp, dp]

@@ -251,6 +251,15 @@ __device__ __forceinline__ void stages(C (&v)[E], C *sm, int ld, int c, int j, c
   }
 }
 
+// Plans with a prescribed number of elements per thread E (T = N/E threads per
+// line); the uneven-ensemble kernels use T = 4 for every size so that one CTA
+// shape serves all of them.  Each radix divides E.
+template <int N, int E> struct PlanE { using R = typename Plan<N>::R; };
+template <> struct PlanE<16, 4> { using R = Radices<4, 4>; };
+template <> struct PlanE<24, 6> { using R = Radices<2, 2, 2, 3>; };
+template <> struct PlanE<40, 10> { using R = Radices<2, 2, 2, 5>; };
+template <> struct PlanE<64, 16> { using R = Radices<8, 8>; };
+
 template <typename C, int N, int E, int DIR, int TWS, int... Rs>
 __device__ __forceinline__ void fft_run(Radices<Rs...>, C (&v)[E], C *sm, int ld, int c, int j,
                                         const C *tw) {
@@ -262,6 +271,12 @@ template <typename C, int N, int DIR, int TWS>
 __device__ __forceinline__ void fft_line(C (&v)[Plan<N>::E], C *sm, int ld, int c, int j,
                                          const C *tw) {
   fft_run<C, N, Plan<N>::E, DIR, TWS>(typename Plan<N>::R{}, v, sm, ld, c, j, tw);
+}
+
+// Same with E taken from the register array (plan PlanE<N, E>).
+template <typename C, int N, int DIR, int TWS, int E>
+__device__ __forceinline__ void fft_line_e(C (&v)[E], C *sm, int ld, int c, int j, const C *tw) {
+  fft_run<C, N, E, DIR, TWS>(typename PlanE<N, E>::R{}, v, sm, ld, c, j, tw);
 }
 
 }  // namespace opfc
