@@ -191,12 +191,8 @@ def timed_steps(model, steps, warmup, ws, stream):
     e1.synchronize()
     model.sync()
     torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    if ws > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms = float(t.item())
-    return ms
+    from openpfc_b200.parallel_plan import max_over_ranks
+    return max_over_ranks(e0.elapsed_time(e1), device="cuda")
 
 
 def run_b200(args):
