@@ -482,10 +482,10 @@ int opfc_ensemble_step(opfc_ensemble *e, int n_steps) {
   if (!e->initialized) return efail(e, OPFC_ERR_STATE, "opfc_ensemble_step before initialize");
   for (int i = 0; i < e->count; ++i)
     if (!e->have_state[i]) return efail(e, OPFC_ERR_STATE, "instance %d has no state", i);
-  if (n_steps == 0) return OPFC_OK;
   ECUDA(e, cudaSetDevice(e->device));
   int rc;
   if (!e->a_valid && (rc = prepare_a(e))) return rc;
+  if (n_steps == 0) return OPFC_OK;  // step(0) only prepares the work arrays
   if (!e->graph || e->graph_steps != n_steps) {
     drop_graph(e);
     // the whole n-step loop is one graph: 5 kernels per step

@@ -1161,10 +1161,20 @@ int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, do
     double c[3];
     for (int a = 0; a < 3; ++a) c[a] = mt_unit(g) * n[a];
     const double R2 = radius_cells * radius_cells;
-    size_t idx = 0;
-    for (int k = 0; k < n[2]; ++k)
-      for (int j = 0; j < n[1]; ++j)
-        for (int i = 0; i < n[0]; ++i, ++idx) {
+    // visit only the (periodically wrapped) bounding box of the sphere
+    int lo[3], cnt[3];
+    for (int a = 0; a < 3; ++a) {
+      lo[a] = (int)std::floor(c[a] - radius_cells) - 1;
+      cnt[a] = std::min(n[a], (int)std::ceil(c[a] + radius_cells) + 2 - lo[a]);
+      if (cnt[a] == n[a]) lo[a] = 0;
+    }
+    for (int kk = 0; kk < cnt[2]; ++kk)
+      for (int jj = 0; jj < cnt[1]; ++jj)
+        for (int ii = 0; ii < cnt[0]; ++ii) {
+          const int i = ((lo[0] + ii) % n[0] + n[0]) % n[0];
+          const int j = ((lo[1] + jj) % n[1] + n[1]) % n[1];
+          const int k = ((lo[2] + kk) % n[2] + n[2]) % n[2];
+          const size_t idx = (size_t)i + (size_t)n[0] * ((size_t)j + (size_t)n[1] * k);
           double d[3] = {i - c[0], j - c[1], k - c[2]};
           for (int a = 0; a < 3; ++a) {  // periodic minimum image
             if (d[a] > 0.5 * n[a]) d[a] -= n[a];

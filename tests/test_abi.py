@@ -75,6 +75,11 @@ def test_ic_generators_match_oracle(oracle):
     dx = [math.pi / 4] * 3
     np.testing.assert_array_equal(ob.ic_seeds(n, dx, -0.1, 0.001, 3, 3.0, 0.2, 9),
                                   oracle.ic_seeds(n, dx, -0.1, 0.001, 3, 3.0, 0.2, 9))
+    # seeds straddling the periodic boundary, radius well below the box
+    for seed in (1, 2, 3):
+        m = (48, 40, 32)
+        np.testing.assert_array_equal(ob.ic_seeds(m, dx, -0.1, 0.001, 6, 7.5, 0.2, seed),
+                                      oracle.ic_seeds(m, dx, -0.1, 0.001, 6, 7.5, 0.2, seed))
     d = 1.1107207345395915
     origin = [-0.5 * d * 16] * 3
     a = ob.ic_seed(np.full((16, 16, 16), -0.4), [d] * 3, origin, [0, 0, 0], 8.0, -0.047, 0.215936)
