@@ -76,13 +76,15 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 constexpr int kMaxDynSmem = 232448;  // 227 KB opt-in per CTA on sm_100
 
-template <typename Real, int N, int W, int MODE, int MODEL> struct TmaCfg {
+template <typename Real, int N, int W, int MODE, int MODEL, bool RADIAL = false> struct TmaCfg {
   using C = typename Cx<Real>::T;
   static constexpr bool UPD = MODE == COL_UPDATE;
   static constexpr bool CHI = UPD && MODEL != MK_PLAIN;
   static constexpr size_t TILE_C = size_t(N) * W * sizeof(C);
   static constexpr size_t TILE_R = size_t(N) * W * sizeof(Real);
-  static constexpr size_t STAGE = TILE_C + (UPD ? TILE_C + 2 * TILE_R + (CHI ? TILE_R : 0) : 0);
+  // radial operators are read from an L2-resident table instead of being staged
+  static constexpr size_t STAGE =
+      TILE_C + (UPD ? TILE_C + (RADIAL ? 0 : 2 * TILE_R + (CHI ? TILE_R : 0)) : 0);
   static constexpr size_t TW = align128(size_t(N) * sizeof(C));
   static constexpr int S0 = int((kMaxDynSmem - TW - 128) / STAGE);
   static constexpr int STAGES = S0 > 3 ? 3 : S0;
@@ -91,15 +93,30 @@ template <typename Real, int N, int W, int MODE, int MODEL> struct TmaCfg {
   static constexpr int NB = N / RB;
 };
 
+// Radial operator lookup: kx <= M unfolded, ky / kz folded to |k|.
+template <typename Real>
+__device__ __forceinline__ void radial_ops(const ColArgs<Real> &a, int kx, int ky, int kz, Real &la, Real &lb,
+                                           Real &ch) {
+  using C = typename Cx<Real>::T;
+  const int fy = ky <= a.rad_n1 / 2 ? ky : a.rad_n1 - ky;
+  const int fz = kz <= a.rad_n2 / 2 ? kz : a.rad_n2 - kz;
+  const int m = kx * kx + fy * fy + fz * fz;
+  const C o = __ldg(reinterpret_cast<const C *>(a.rad_ops) + m);
+  la = o.x;
+  lb = o.y;
+  ch = a.rad_chi ? __ldg(a.rad_chi + m) : Real(1);
+}
+
 // Tensor maps: PLAIN uses m0 (array set 0) and m1 (array set 1); UPDATE uses
-// m0 = N_hat partial (A), m1 = psi_hat, m2 = tab_a, m3 = tab_b, m4 = tab_chi.
-template <typename Real, int N, int W, int MODE, int DIR, int MODEL, bool INV>
+// m0 = N_hat partial (A), m1 = psi_hat, m2 = tab_a, m3 = tab_b, m4 = tab_chi
+// (m2..m4 unused with RADIAL).
+template <typename Real, int N, int W, int MODE, int DIR, int MODEL, bool INV, bool RADIAL>
 __global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
     col_tma_kernel(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
                    const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3,
                    const __grid_constant__ CUtensorMap m4, const ColArgs<Real> a, const int axis,
                    unsigned *flag) {
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL>;
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, RADIAL>;
   using C = typename Cx<Real>::T;
   constexpr int E = Plan<N>::E;
   constexpr int T = N / E;
@@ -141,6 +158,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
       if constexpr (UPD) {
         const size_t offr = size_t(b) * Cfg::RB * W * sizeof(Real);
         tma_load_3d(st + Cfg::TILE_C + offc, &m1, &bars[s], ti * W * 2, y, z);
+        if constexpr (RADIAL) continue;
         tma_load_3d(st + 2 * Cfg::TILE_C + offr, &m2, &bars[s], ti * W, y, z);
         tma_load_3d(st + 2 * Cfg::TILE_C + Cfg::TILE_R + offr, &m3, &bars[s], ti * W, y, z);
         if constexpr (Cfg::CHI)
@@ -194,10 +212,17 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
       for (int m = 0; m < E; ++m) {
         const int e = (j + T * m) * W + c;
         const C p = tpsi[e];
-        const Real la = ta[e], lb = tb[e];
+        Real la, lb, ch = Real(1);
+        if constexpr (RADIAL) {
+          radial_ops(a, ti * W + c, to, j + T * m, la, lb, ch);  // z pass: ky = to, kz = p
+        } else {
+          la = ta[e];
+          lb = tb[e];
+          if constexpr (Cfg::CHI) ch = tc[e];
+        }
         const C np = mk<C>(la * p.x + lb * v[m].x, la * p.y + lb * v[m].y);
         ph[base + (long long)(j + T * m) * fs] = np;
-        if constexpr (Cfg::CHI) w[m] = cscale(np, tc[e]);
+        if constexpr (Cfg::CHI) w[m] = cscale(np, ch);
         v[m] = np;
       }
       if constexpr (INV) {
@@ -264,13 +289,21 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
       for (int m = 0; m < E; ++m) {
         const long long idx = base + (long long)(j + T * m) * fs;
         C np = mk<C>(0, 0);
+        Real ch = Real(1);
         if (ok) {
           const C p = ph[idx];
-          const Real la = a.tab_a[idx], lb = a.tab_b[idx];
+          Real la, lb;
+          if constexpr (RADIAL) {
+            radial_ops(a, a.rad_M, cg, j + T * m, la, lb, ch);  // Nyquist plane: kx = M, ky = column
+          } else {
+            la = a.tab_a[idx];
+            lb = a.tab_b[idx];
+            if constexpr (Cfg::CHI) ch = a.tab_chi[idx];
+          }
           np = mk<C>(la * p.x + lb * v[m].x, la * p.y + lb * v[m].y);
           ph[idx] = np;
         }
-        if constexpr (Cfg::CHI) w[m] = ok ? cscale(np, a.tab_chi[idx]) : mk<C>(0, 0);
+        if constexpr (Cfg::CHI) w[m] = ok ? cscale(np, ch) : mk<C>(0, 0);
         v[m] = np;
       }
       if constexpr (INV) {

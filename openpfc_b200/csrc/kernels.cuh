@@ -30,6 +30,11 @@ template <typename Real> struct ColArgs {
   const void *tw;
   void *psi_hat;
   const Real *tab_a, *tab_b, *tab_chi;
+  // radial operators (isotropic grids): rad_ops[m] = (opL, opN), rad_chi[m],
+  // m = kx^2 + ky^2 + kz^2 in folded integer indices
+  const void *rad_ops;
+  const Real *rad_chi;
+  int rad_M, rad_n1, rad_n2;
 };
 
 template <typename C> __device__ __forceinline__ C czero() { return mk<C>(0, 0); }
@@ -512,17 +517,17 @@ static inline ColSeg retile(ColSeg g, int W, int Wold) {
   return g;
 }
 
-template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, bool RADIAL>
 static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
   using C = typename Cx<Real>::T;
   constexpr int W = tma_col_width(N, (int)sizeof(C), MODE);
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL>;
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, RADIAL>;
   if constexpr (Cfg::STAGES < 1) {
     return -1;
   } else {
     if (L.seg[0].ncols % W != 0 || L.seg[0].col_stride != 1) return -1;
     constexpr int NT = W * (N / Plan<N>::E);
-    auto k = col_tma_kernel<Real, N, W, MODE, DIR, MODEL, INV>;
+    auto k = col_tma_kernel<Real, N, W, MODE, DIR, MODEL, INV, RADIAL>;
     static bool attr = false;
     if (!attr) {
       cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
@@ -540,6 +545,11 @@ static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
     a.tab_a = reinterpret_cast<const Real *>(L.tab_a);
     a.tab_b = reinterpret_cast<const Real *>(L.tab_b);
     a.tab_chi = reinterpret_cast<const Real *>(L.tab_chi);
+    a.rad_ops = L.rad_ops;
+    a.rad_chi = reinterpret_cast<const Real *>(L.rad_chi);
+    a.rad_M = L.rad_M;
+    a.rad_n1 = L.rad_n1;
+    a.rad_n2 = L.rad_n2;
     const CUtensorMap *t0 = reinterpret_cast<const CUtensorMap *>(L.tmap[0]);
     auto pick = [&](int i) { return L.tmap[i] ? *reinterpret_cast<const CUtensorMap *>(L.tmap[i]) : *t0; };
     int G = L.num_sms > 0 ? L.num_sms : 148;
@@ -556,7 +566,12 @@ template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
 static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
   using C = typename Cx<Real>::T;
   if (L.tmap[0]) {
-    const int rc = launch_col_tma<Real, N, MODE, DIR, MODEL, INV>(L, s);
+    int rc;
+    if constexpr (MODE == COL_UPDATE)
+      rc = L.rad_ops ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, true>(L, s)
+                     : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, false>(L, s);
+    else
+      rc = launch_col_tma<Real, N, MODE, DIR, MODEL, INV, false>(L, s);
     if (rc >= 0) return rc;
   }
   constexpr int W = Width<Real>::W;

@@ -52,6 +52,12 @@ struct ColLaunch {
   // PLAIN: tmap[0], tmap[1] = input of array set 0 / 1; UPDATE: A, psi_hat,
   // tab_a, tab_b, tab_chi.  tmap[0] == nullptr selects the direct-load kernel.
   const void *tmap[5];
+  // COL_UPDATE on isotropic grids: operators indexed by m = kx^2 + ky^2 + kz^2
+  // (folded integer indices) instead of per-mode tables; rad_ops holds (opL, opN)
+  // pairs in the compute precision, rad_chi the filter (or nullptr)
+  const void *rad_ops;
+  const void *rad_chi;
+  int rad_M, rad_n1, rad_n2;
   int axis;            // 1 = y, 2 = z
   unsigned int *flag;  // bit 1: a bounded wait expired
   int num_sms;

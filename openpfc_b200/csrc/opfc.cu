@@ -114,6 +114,8 @@ struct opfc_handle {
   int ckpt_K = 0, ckpt_steps = 0;
   std::vector<void *> seg;   // psi_hat of each step of one recomputed segment
   void *tab_ar = nullptr, *tab_br = nullptr;
+  // isotropic grids: (opL, opN) and the filter as functions of m = |k_index|^2
+  void *rad_ops = nullptr, *rad_chi = nullptr;
   void *adj_c[2] = {nullptr, nullptr};
   void *adj_r[3] = {nullptr, nullptr, nullptr};
 
@@ -442,10 +444,20 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     if (h->use_tma && Z.N > 1 && h->M % W == 0) {
       Z.tmap[0] = tmap_for(h, h->work_a, 2, W, false);
       Z.tmap[1] = tmap_for(h, h->psi_hat, 2, W, false);
-      Z.tmap[2] = tmap_for(h, h->tab_a, 2, W, true);
-      Z.tmap[3] = tmap_for(h, h->tab_b, 2, W, true);
-      Z.tmap[4] = h->tab_chi ? tmap_for(h, h->tab_chi, 2, W, true) : nullptr;
-      if (!Z.tmap[1] || !Z.tmap[2] || !Z.tmap[3] || (h->tab_chi && !Z.tmap[4])) Z.tmap[0] = nullptr;
+      if (h->rad_ops) {
+        // isotropic grid: operators from the L2-resident radial tables
+        Z.rad_ops = h->rad_ops;
+        Z.rad_chi = h->rad_chi;
+        Z.rad_M = h->M;
+        Z.rad_n1 = h->n1;
+        Z.rad_n2 = h->n2;
+        if (!Z.tmap[1]) Z.tmap[0] = nullptr;
+      } else {
+        Z.tmap[2] = tmap_for(h, h->tab_a, 2, W, true);
+        Z.tmap[3] = tmap_for(h, h->tab_b, 2, W, true);
+        Z.tmap[4] = h->tab_chi ? tmap_for(h, h->tab_chi, 2, W, true) : nullptr;
+        if (!Z.tmap[1] || !Z.tmap[2] || !Z.tmap[3] || (h->tab_chi && !Z.tmap[4])) Z.tmap[0] = nullptr;
+      }
     }
     LAUNCH_TRY(h, col(h, Z));
   }
@@ -722,7 +734,8 @@ int opfc_destroy(opfc_handle *h) {
     if (p) cudaFree(p);
   for (void *p : h->seg)
     if (p) cudaFree(p);
-  void *adj[] = {h->tab_ar, h->tab_br, h->adj_c[0], h->adj_c[1], h->adj_r[0], h->adj_r[1], h->adj_r[2]};
+  void *adj[] = {h->tab_ar,   h->tab_br,   h->adj_c[0], h->adj_c[1], h->adj_r[0],
+                 h->adj_r[1], h->adj_r[2], h->rad_ops,  h->rad_chi};
   for (void *p : adj)
     if (p) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -867,6 +880,58 @@ int opfc_initialize(opfc_handle *h, double dt) {
   if ((rc = upload(ta, &h->tab_a))) return rc;
   if ((rc = upload(tb, &h->tab_b))) return rc;
   if (need_chi && (rc = upload(tc, &h->tab_chi))) return rc;
+
+  // Isotropic grids (one frequency step f on all axes): every operator depends
+  // only on m = i^2 + j^2 + k^2 of the folded integer indices (k^2 = f^2 m), so
+  // the fused z update reads small L2-resident tables instead of streaming the
+  // per-mode tables from HBM.  Same formulas, FP64, rounded once.
+  const char *no_rad = std::getenv("OPFC_NO_RADIAL");
+  if (f0 == f1 && f1 == f2 && !(no_rad && no_rad[0] == '1')) {
+    const long mmax = (long)(n0 / 2) * (n0 / 2) + (long)(n1 / 2) * (n1 / 2) + (long)(n2 / 2) * (n2 / 2);
+    const size_t cnt = (size_t)mmax + 1;
+    std::vector<double> ops(2 * cnt), chi(need_chi ? cnt : 0);
+    parallel_for((long)cnt, [&](long m) {
+      const double k2 = f0 * f0 * (double)m;
+      if (model == OPFC_MODEL_TUNGSTEN) {
+        const double kLap = -k2;
+        const double fMF = std::exp(kLap / lambda2);
+        const double kv = std::sqrt(-kLap) - 1.0;
+        const double kk = kv * kv;
+        const double g1 = (P.alpha_highOrd == 0)
+                              ? std::exp(-kk / alpha2)
+                              : std::exp(-(kk + rTol * std::pow(kv, P.alpha_highOrd)) / alpha2);
+        const double g2 = 1.0 - 1.0 / alpha2 * kk;
+        const double opCk = P.stabP + p2b - peak * ((kv < 0.0) ? g1 : g2) + q2b * fMF;
+        const double L = kLap * opCk;
+        const double arg = L * dt;
+        const double phi1 = (std::fabs(L) < 1e-12) ? dt + 0.5 * L * dt * dt : std::expm1(arg) / L;
+        ops[2 * m] = std::exp(arg);
+        ops[2 * m + 1] = kLap * phi1;
+        chi[m] = fMF;
+      } else {
+        const double L = -k2 * (r + (1.0 - k2) * (1.0 - k2));
+        const double eL = std::exp(L * dt);
+        ops[2 * m] = eL;
+        ops[2 * m + 1] = (std::fabs(L) > 1e-14) ? (eL - 1.0) / L * (-k2) : dt * (-k2);
+        if (need_chi) chi[m] = std::exp(-k2 / (2.0 * fa * fa));
+      }
+    });
+    auto up = [&](const std::vector<double> &src, void **dst) -> int {
+      if (*dst) cudaFree(*dst);
+      *dst = nullptr;
+      int rc2 = dev_alloc(h, dst, src.size() * h->rsz);
+      if (rc2) return rc2;
+      if (h->prec == OPFC_FP64) {
+        CUDA_TRY(h, cudaMemcpy(*dst, src.data(), src.size() * 8, cudaMemcpyHostToDevice));
+      } else {
+        std::vector<float> f(src.begin(), src.end());
+        CUDA_TRY(h, cudaMemcpy(*dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+      }
+      return OPFC_OK;
+    };
+    if ((rc = up(ops, &h->rad_ops))) return rc;
+    if (need_chi && (rc = up(chi, &h->rad_chi))) return rc;
+  }
   h->dt = dt;
   h->initialized = true;
   h->a_valid = false;

@@ -25,7 +25,9 @@ template <typename Real, int R, int MODEL> struct XSqCfg {
   static constexpr size_t BUF = align128(TILE > EXCH ? TILE : EXCH);
   static constexpr int NARR = MODEL == MK_TUNGSTEN ? 2 : 1;
   static constexpr size_t STAGE = BUF * NARR;
-  static constexpr size_t TW = align128(size_t(2 * M) * sizeof(C));
+  // only W_N0^k for k < M is read per tile (pre/post-processing); the stage-2
+  // table is built from the global table, so 3 CTAs fit per SM
+  static constexpr size_t TW = align128(size_t(M) * sizeof(C));
   static constexpr size_t TWS = align128(size_t(R) * R * sizeof(C));
   static constexpr int STAGES = 2;
   static constexpr size_t SMEM = TW + TWS + STAGES * STAGE + 64;
@@ -75,7 +77,7 @@ __global__ void __launch_bounds__(Width<Real>::W *R) x_sq_kernel(const XArgs<Rea
   const int lane = tid & 31;
   const int partner = (lane & ~(R - 1)) | ((R - j) & (R - 1));
   const C *gtw = reinterpret_cast<const C *>(a.tw);
-  for (int i = tid; i < N0; i += NT) tw[i] = gtw[i];
+  for (int i = tid; i < M; i += NT) tw[i] = gtw[i];
   for (int i = tid; i < (R - 1) * R; i += NT) {
     const int r = i / R + 1, k = i % R;
     tws[i] = gtw[(2 * k * r) % N0];  // W_M^{k r} = exp(-2 pi i k r / M)

@@ -14,12 +14,17 @@ pytestmark = pytest.mark.gpu
 PI4 = [math.pi / 4] * 3
 
 
-@pytest.fixture(params=["tma", "direct"])
+@pytest.fixture(params=["tma", "tma_tables", "direct"])
 def path(request, monkeypatch):
+    """tma: pipelined kernels with radial operator tables on isotropic grids;
+    tma_tables: pipelined kernels streaming the per-mode tables (OPFC_NO_RADIAL=1);
+    direct: direct-load kernels (OPFC_NO_TMA=1)."""
+    monkeypatch.delenv("OPFC_NO_TMA", raising=False)
+    monkeypatch.delenv("OPFC_NO_RADIAL", raising=False)
     if request.param == "direct":
         monkeypatch.setenv("OPFC_NO_TMA", "1")
-    else:
-        monkeypatch.delenv("OPFC_NO_TMA", raising=False)
+    elif request.param == "tma_tables":
+        monkeypatch.setenv("OPFC_NO_RADIAL", "1")
     return request.param
 
 
