@@ -201,6 +201,17 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
 #pragma unroll
       for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
     } else {
+      // radial operators: gather from L2 before the transform so the loads
+      // overlap it (z pass: kx = column, ky = outer index, kz = p)
+      Real rla[RADIAL ? E : 1], rlb[RADIAL ? E : 1], rch[RADIAL && Cfg::CHI ? E : 1];
+      if constexpr (RADIAL) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          Real ch;
+          radial_ops(a, ti * W + c, to, j + T * m, rla[m], rlb[m], ch);
+          if constexpr (Cfg::CHI) rch[m] = ch;
+        }
+      }
       fft_line<C, N, -1, N>(v, tin, W, c, j, tw);
       const C *tpsi = reinterpret_cast<const C *>(st + Cfg::TILE_C);
       const Real *ta = reinterpret_cast<const Real *>(st + 2 * Cfg::TILE_C);
@@ -214,7 +225,9 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
         const C p = tpsi[e];
         Real la, lb, ch = Real(1);
         if constexpr (RADIAL) {
-          radial_ops(a, ti * W + c, to, j + T * m, la, lb, ch);  // z pass: ky = to, kz = p
+          la = rla[m];
+          lb = rlb[m];
+          if constexpr (Cfg::CHI) ch = rch[m];
         } else {
           la = ta[e];
           lb = tb[e];
