@@ -211,6 +211,7 @@ def run_b200(args):
 
     m = ob.PfcB200((N, N, N), DX, r=R, precision=ob.FP32, device=local)
     m.initialize(DT)
+    tune32 = m.autotune()  # kernel variant per pass, timed on this GPU (untimed set-up)
     m.set_psi(psi0_32)
     stream = torch.cuda.ExternalStream(m.stream, device=torch.device("cuda", local))
     # clocks are sampled from the warm-up through the end of the timed region
@@ -224,6 +225,7 @@ def run_b200(args):
     if not args.no_fp64:
         m64 = ob.PfcB200((N, N, N), DX, r=R, precision=ob.FP64, device=local)
         m64.initialize(DT)
+        m64.autotune()
         m64.set_psi(psi0_32.astype(np.float64))
         s64 = max(3, min(args.steps, 20))
         ms64 = timed_steps(m64, s64, min(args.warmup, 3), ws, torch.cuda.ExternalStream(
@@ -310,7 +312,8 @@ def run_b200(args):
                            "l2": "inputs larger than L2 (0.54 GB arrays), no flush",
                            "parallelism": f"replicas x{ws}"},
                 "e2e": e2e, "roofline": roofline, "passes": passes, "cpu_baseline": cpu,
-                "clocks": ck.summary(), "gpu_launches": kps * args.steps}
+                "clocks": ck.summary(), "gpu_launches": kps * args.steps,
+                "autotune": {"variants_yxz": m.variants(), "ms": tune32}}
         line.update(extra)
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -331,6 +334,7 @@ def run_filtered(args):
     t_ic = time.time() - t0
     m = ob.FilteredB200((n, n, n), DX, r=-0.3, alpha=0.5, p2=-0.1, p3=-0.5, p4=0.3, precision=ob.FP32)
     m.initialize(DT)
+    tune = m.autotune()
     m.set_psi(psi0)
     del psi0
     stream = torch.cuda.ExternalStream(m.stream)
@@ -348,7 +352,7 @@ def run_filtered(args):
             "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"mean-field-filtered PFC {n}^3 FP32, 8 seeds", "ic_seconds": t_ic},
             "alg_bytes_per_step": sum(ab.values()), "passes": passes, "peak": hbm, "peak_kind": peak_kind,
-            "clocks": ck.summary()}
+            "clocks": ck.summary(), "autotune": {"variants_yxz": m.variants(), "ms": tune}}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -144,6 +144,20 @@ int opfc_profile_step(opfc_handle *h, int reps, double *ms, int max_kernels);
 /* Name of kernel k of the step ("y_inverse", "x_fused", ...). */
 const char *opfc_step_kernel_name(int k);
 
+/* Autotuner (replaces pfc::gpu::AutoTuner::tune_kernel,
+ * include/openpfc/runtime/common/gpu_autotune.hpp:295-333, same environment
+ * variables OPENPFC_GPU_AUTOTUNE_{DISABLE,MODE,CACHE_DIR}): times the kernel
+ * variants of each pass of the step (y: pipelined | direct; x: pipelined |
+ * direct; z update: pipelined with streamed tables | pipelined with radial
+ * tables (isotropic grids) | direct; 3 warm-up + 10 timed launches each), keeps
+ * the fastest and caches it per device; opfc_initialize applies cached choices.
+ * ms (7 doubles, may be NULL) receives the mean milliseconds per launch of
+ * y0 y1 x0 x1 z0 z1 z2 (-1 if not applicable).  Call after opfc_initialize; the
+ * passes run in place, so set the field afterwards.  opfc_variants reports the
+ * chosen (y, x, z) variants. */
+int opfc_autotune(opfc_handle *h, double *ms);
+int opfc_variants(const opfc_handle *h, int *var);
+
 /* Adjoint of the plain model (no counterpart in the reference, which has no
  * differentiation).  opfc_set_r changes r (PLAIN/FILTERED) and rebuilds the
  * tables.  opfc_forward_checkpointed advances n_steps from the current state,

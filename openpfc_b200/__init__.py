@@ -207,6 +207,19 @@ class _ModelBase(_Handle):
     def kernels_per_step(self) -> int:
         return int(lib().opfc_kernels_per_step(self._h))
 
+    def autotune(self) -> dict:
+        """Time every kernel variant of each pass, keep the fastest (cached per
+        device); returns ms per launch by variant.  Set the field afterwards."""
+        ms = (ctypes.c_double * 7)()
+        _check(self._h, lib().opfc_autotune(self._h, ms))
+        names = ["y.pipelined", "y.direct", "x.pipelined", "x.direct", "z.tables", "z.radial", "z.direct"]
+        return dict(zip(names, list(ms)))
+
+    def variants(self) -> tuple:
+        v = (ctypes.c_int * 3)()
+        _check(self._h, lib().opfc_variants(self._h, v))
+        return tuple(v)
+
     def profile_step(self, reps: int = 10) -> dict:
         """Mean ms per launch of each kernel of the step, timed alone with CUDA
         events on the handle's stream.  Leaves the field undefined."""

@@ -121,6 +121,8 @@ def lib():
     L.opfc_ensemble_cells.restype = sz
     L.opfc_ensemble_stream.argtypes = [H]
     L.opfc_ensemble_stream.restype = vp
+    L.opfc_autotune.argtypes = [H, dp]
+    L.opfc_variants.argtypes = [H, ip]
     L.opfc_set_r.argtypes = [H, cd]
     L.opfc_forward_checkpointed.argtypes = [H, ci, ci]
     L.opfc_adjoint.argtypes = [H, vp, ci, ci, vp, dp, dp]

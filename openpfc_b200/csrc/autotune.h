@@ -34,6 +34,7 @@ class AutoTuner {
   // cached variant index for `key`, or `fallback`
   int get_config(const std::string &key, int fallback) {
     std::lock_guard<std::mutex> lock(mu_);
+    refresh();
     if (disabled_ || mode_ == "fallback_only") return fallback;
     load_once();
     auto it = cache_.find(key);
@@ -44,6 +45,10 @@ class AutoTuner {
   // `run` returns 0 on success; failing candidates are skipped.
   int tune(const std::string &key, int n, const std::function<int(int)> &run, cudaStream_t s,
            std::vector<double> *ms_out = nullptr) {
+    {
+      std::lock_guard<std::mutex> lock(mu_);
+      refresh();
+    }
     if (disabled_ || mode_ == "fallback_only" || mode_ == "cache_only") return get_config(key, 0);
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
@@ -83,13 +88,21 @@ class AutoTuner {
   }
 
  private:
-  AutoTuner() {
+  AutoTuner() { refresh(); }
+
+  // the environment is read on every call, so a process can redirect the cache
+  void refresh() {
     const char *d = std::getenv("OPENPFC_GPU_AUTOTUNE_DISABLE");
     disabled_ = d && std::string(d) == "1";
     const char *m = std::getenv("OPENPFC_GPU_AUTOTUNE_MODE");
     mode_ = m ? m : "auto";
     const char *c = std::getenv("OPENPFC_GPU_AUTOTUNE_CACHE_DIR");
-    dir_ = c ? c : ".";
+    const std::string dir = c ? c : ".";
+    if (dir != dir_) {
+      dir_ = dir;
+      loaded_ = false;
+      cache_.clear();
+    }
   }
 
   std::string path() const {

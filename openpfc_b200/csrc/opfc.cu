@@ -27,6 +27,7 @@
 #include "fft_core.cuh"
 #include "launch.h"
 #include "twiddle.h"
+#include "autotune.h"
 
 using namespace opfc;
 
@@ -123,6 +124,10 @@ struct opfc_handle {
   cudaGraphExec_t graph_exec = nullptr;
 
   bool use_tma = true;  // TMA-fed column passes (OPFC_NO_TMA=1 disables)
+  // kernel variants per pass, chosen by the autotuner (see opfc_autotune):
+  // var_y: 0 pipelined, 1 direct; var_x: 0 pipelined, 1 direct;
+  // var_z: 0 pipelined with streamed tables, 1 pipelined with radial tables, 2 direct
+  int var_y = 0, var_x = 0, var_z = 0;
   int num_sms = 148;
   struct Tmap {
     const void *ptr;
@@ -288,7 +293,7 @@ int col_plain(opfc_handle *h, int axis, int dir, const void *in0, void *out0,
   L.tw = axis == 1 ? h->tw_y : h->tw_z;
   L.axis = axis;
   const int W = tma_col_width(L.N, 2 * (int)h->rsz, COL_PLAIN);
-  if (h->use_tma && L.N > 1 && h->M % W == 0) {
+  if (h->use_tma && h->var_y == 0 && L.N > 1 && h->M % W == 0) {
     L.tmap[0] = tmap_for(h, in0, axis, W, false);
     L.tmap[1] = in1 ? tmap_for(h, in1, axis, W, false) : nullptr;
     if (in1 && !L.tmap[1]) L.tmap[0] = nullptr;
@@ -338,12 +343,22 @@ XLaunch x_base(opfc_handle *h) {
   L.scale = 1.0 / ((double)h->n0 * h->n1 * h->n2);
   L.mean = 0.0;
   L.flag = h->flag;
-  L.use_tma = h->use_tma;
+  L.use_tma = h->use_tma && h->var_x == 0;
   L.num_sms = h->num_sms;
   return L;
 }
 
 double mean_density(const opfc_handle *h) { return h->mass_sum / (double)h->nr; }
+
+// autotuner cache key of one pass of this handle's step
+std::string tune_key(const opfc_handle *h, const char *pass) {
+  static const char *models[] = {"plain", "tungsten", "filtered"};
+  char b[160];
+  std::snprintf(b, sizeof b, "step/%s/%s/%dx%dx%d/%s/f%s", h->prec == OPFC_FP64 ? "fp64" : "fp32",
+                models[h->desc.model], h->n0, h->n1, h->n2, pass,
+                (h->desc.dx[0] == h->desc.dx[1] && h->desc.dx[1] == h->desc.dx[2]) ? "iso" : "aniso");
+  return b;
+}
 
 // A <- F_z^-1[psi_hat] (and, for TUNGSTEN, B <- F_z^-1[chi psi_hat]); FILTERED
 // keeps only the filtered density in A.
@@ -441,10 +456,10 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.tab_chi = h->tab_chi;
     Z.axis = 2;
     const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE);
-    if (h->use_tma && Z.N > 1 && h->M % W == 0) {
+    if (h->use_tma && h->var_z != 2 && Z.N > 1 && h->M % W == 0) {
       Z.tmap[0] = tmap_for(h, h->work_a, 2, W, false);
       Z.tmap[1] = tmap_for(h, h->psi_hat, 2, W, false);
-      if (h->rad_ops) {
+      if (h->rad_ops && h->var_z == 1) {
         // isotropic grid: operators from the L2-resident radial tables
         Z.rad_ops = h->rad_ops;
         Z.rad_chi = h->rad_chi;
@@ -933,6 +948,13 @@ int opfc_initialize(opfc_handle *h, double dt) {
     if (need_chi && (rc = up(chi, &h->rad_chi))) return rc;
   }
   h->dt = dt;
+  // kernel variants: the autotuner's cached choice, else the defaults;
+  // OPFC_Z_VARIANT forces the z-update variant (0 tables, 1 radial, 2 direct)
+  h->var_y = AutoTuner::instance().get_config(tune_key(h, "y"), 0);
+  h->var_x = AutoTuner::instance().get_config(tune_key(h, "x"), 0);
+  h->var_z = AutoTuner::instance().get_config(tune_key(h, "z"), 0);
+  if (const char *zv = std::getenv("OPFC_Z_VARIANT")) h->var_z = std::atoi(zv);
+  if (h->var_z == 1 && !h->rad_ops) h->var_z = 0;
   h->initialized = true;
   h->a_valid = false;
   release_graph(h);
@@ -1141,6 +1163,45 @@ size_t opfc_size_outbox(const opfc_handle *h) { return h ? h->nc : 0; }
 size_t opfc_allocated_bytes(const opfc_handle *h) { return h ? h->allocated : 0; }
 void *opfc_get_stream(const opfc_handle *h) { return h ? (void *)h->stream : nullptr; }
 int opfc_kernels_per_step(const opfc_handle *h) { return h ? kStepKernels : 0; }
+
+int opfc_autotune(opfc_handle *h, double *ms) {
+  if (!h) return OPFC_ERR_ARG;
+  if (!h->initialized) return fail(h, OPFC_ERR_STATE, "opfc_autotune needs the operator tables");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  release_graph(h);
+  AutoTuner &T = AutoTuner::instance();
+  std::vector<double> my, mx, mz;
+  // each candidate runs its pass alone, in place on whatever the arrays hold
+  h->var_y = T.tune(tune_key(h, "y"), 2, [&](int v) { h->var_y = v; return enqueue_step(h, 0); }, h->stream, &my);
+  h->var_x = T.tune(tune_key(h, "x"), 2, [&](int v) { h->var_x = v; return enqueue_step(h, 1); }, h->stream, &mx);
+  h->var_z = T.tune(
+      tune_key(h, "z"), 3,
+      [&](int v) {
+        if (v == 1 && !h->rad_ops) return (int)OPFC_ERR_ARG;
+        h->var_z = v;
+        return enqueue_step(h, 3);
+      },
+      h->stream, &mz);
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  cudaMemset(h->flag, 0, sizeof(unsigned int));
+  h->have_state = false;  // the passes overwrote the state
+  h->a_valid = false;
+  if (ms) {
+    const std::vector<double> *all[3] = {&my, &mx, &mz};
+    int o = 0;
+    for (int p = 0; p < 3; ++p)
+      for (int v = 0; v < (p == 2 ? 3 : 2); ++v) ms[o++] = (int)all[p]->size() > v ? (*all[p])[v] : -1.0;
+  }
+  return OPFC_OK;
+}
+
+int opfc_variants(const opfc_handle *h, int *var) {
+  if (!h || !var) return OPFC_ERR_ARG;
+  var[0] = h->var_y;
+  var[1] = h->var_x;
+  var[2] = h->var_z;
+  return OPFC_OK;
+}
 
 int opfc_profile_step(opfc_handle *h, int reps, double *ms, int max_kernels) {
   if (!h || !ms || reps < 1) return OPFC_ERR_ARG;

@@ -14,17 +14,19 @@ pytestmark = pytest.mark.gpu
 PI4 = [math.pi / 4] * 3
 
 
-@pytest.fixture(params=["tma", "tma_tables", "direct"])
+@pytest.fixture(params=["tma", "tma_radial", "direct"])
 def path(request, monkeypatch):
-    """tma: pipelined kernels with radial operator tables on isotropic grids;
-    tma_tables: pipelined kernels streaming the per-mode tables (OPFC_NO_RADIAL=1);
+    """tma: pipelined kernels streaming the per-mode tables (default);
+    tma_radial: the z update reading radial operator tables (OPFC_Z_VARIANT=1,
+    isotropic grids; others fall back to tables);
     direct: direct-load kernels (OPFC_NO_TMA=1)."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
-    monkeypatch.delenv("OPFC_NO_RADIAL", raising=False)
+    monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
+    monkeypatch.setenv("OPENPFC_GPU_AUTOTUNE_MODE", "fallback_only")
     if request.param == "direct":
         monkeypatch.setenv("OPFC_NO_TMA", "1")
-    elif request.param == "tma_tables":
-        monkeypatch.setenv("OPFC_NO_RADIAL", "1")
+    elif request.param == "tma_radial":
+        monkeypatch.setenv("OPFC_Z_VARIANT", "1")
     return request.param
 
 
@@ -73,6 +75,30 @@ def test_tungsten(oracle, path, prec, tol, n):
     m.step(5)
     m.sync()
     assert rel_l2(m.get_psi(), ref) <= tol
+
+
+def test_autotune_then_parity(oracle, tmp_path, monkeypatch):
+    """The autotuner times every variant, picks one, and the tuned step still
+    matches the oracle; a second handle reads the cached choice."""
+    monkeypatch.setenv("OPENPFC_GPU_AUTOTUNE_CACHE_DIR", str(tmp_path))
+    monkeypatch.delenv("OPENPFC_GPU_AUTOTUNE_MODE", raising=False)
+    monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
+    n = (64, 64, 64)
+    psi0 = oracle.ic_noise(n, -0.285, 0.01, 21)
+    ref = oracle.run_plain(psi0, PI4, -0.25, 0.5, 10)
+    m = ob.PfcB200(n, PI4, precision=ob.FP32)
+    m.initialize(0.5)
+    ms = m.autotune()
+    assert ms["y.pipelined"] > 0 and ms["z.tables"] > 0 and ms["z.radial"] > 0
+    chosen = m.variants()
+    m.set_psi(psi0)
+    m.step(10)
+    m.sync()
+    assert rel_l2(m.get_psi(), ref) <= 1e-5
+    assert any(f.name.endswith("_opfc_autotune.json") for f in tmp_path.iterdir())
+    m2 = ob.PfcB200(n, PI4, precision=ob.FP32)
+    m2.initialize(0.5)
+    assert m2.variants() == chosen
 
 
 def test_transforms(oracle, path):
