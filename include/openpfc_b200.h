@@ -147,14 +147,18 @@ const char *opfc_step_kernel_name(int k);
 /* Autotuner (replaces pfc::gpu::AutoTuner::tune_kernel,
  * include/openpfc/runtime/common/gpu_autotune.hpp:295-333, same environment
  * variables OPENPFC_GPU_AUTOTUNE_{DISABLE,MODE,CACHE_DIR}): times the kernel
- * variants of each pass of the step (y: pipelined | direct; x: pipelined |
- * direct; z update: pipelined with streamed tables | pipelined with radial
- * tables (isotropic grids) | direct; 3 warm-up + 10 timed launches each), keeps
- * the fastest and caches it per device; opfc_initialize applies cached choices.
- * ms (7 doubles, may be NULL) receives the mean milliseconds per launch of
- * y0 y1 x0 x1 z0 z1 z2 (-1 if not applicable).  Call after opfc_initialize; the
- * passes run in place, so set the field afterwards.  opfc_variants reports the
- * chosen (y, x, z) variants. */
+ * variants of each pass of the step (y: 0 pipelined | 1 direct | 2 pipelined
+ * with half-width tiles, two CTAs per SM; x: 0 pipelined | 1 direct; z update:
+ * 0 pipelined with streamed tables | 1 pipelined with radial tables (isotropic
+ * grids) | 2 direct with streamed tables | 3 pipelined with operators computed
+ * from k^2 | 4 direct with computed operators (3, 4: PLAIN and FILTERED);
+ * 3 warm-up + 10 timed launches each), keeps the fastest and caches it per
+ * device; opfc_initialize applies cached choices.  ms (OPFC_AUTOTUNE_SLOTS
+ * doubles, may be NULL) receives the mean milliseconds per launch of
+ * y0 y1 y2 x0 x1 z0 z1 z2 z3 z4 (-1 if not applicable).  Call after
+ * opfc_initialize; the passes run in place, so set the field afterwards.
+ * opfc_variants reports the chosen (y, x, z) variants. */
+#define OPFC_AUTOTUNE_SLOTS 10
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 

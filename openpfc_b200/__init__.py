@@ -210,9 +210,10 @@ class _ModelBase(_Handle):
     def autotune(self) -> dict:
         """Time every kernel variant of each pass, keep the fastest (cached per
         device); returns ms per launch by variant.  Set the field afterwards."""
-        ms = (ctypes.c_double * 7)()
+        names = ["y.pipelined", "y.direct", "y.narrow", "x.pipelined", "x.direct", "z.tables", "z.radial",
+                 "z.direct", "z.computed", "z.direct_computed"]
+        ms = (ctypes.c_double * len(names))()
         _check(self._h, lib().opfc_autotune(self._h, ms))
-        names = ["y.pipelined", "y.direct", "x.pipelined", "x.direct", "z.tables", "z.radial", "z.direct"]
         return dict(zip(names, list(ms)))
 
     def variants(self) -> tuple:

@@ -76,15 +76,16 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 constexpr int kMaxDynSmem = 232448;  // 227 KB opt-in per CTA on sm_100
 
-template <typename Real, int N, int W, int MODE, int MODEL, bool RADIAL = false> struct TmaCfg {
+template <typename Real, int N, int W, int MODE, int MODEL, int OPS = 0> struct TmaCfg {
   using C = typename Cx<Real>::T;
   static constexpr bool UPD = MODE == COL_UPDATE;
   static constexpr bool CHI = UPD && MODEL != MK_PLAIN;
   static constexpr size_t TILE_C = size_t(N) * W * sizeof(C);
   static constexpr size_t TILE_R = size_t(N) * W * sizeof(Real);
-  // radial operators are read from an L2-resident table instead of being staged
+  // radial operators come from an L2-resident table and computed operators
+  // from k^2: only the per-mode tables are staged
   static constexpr size_t STAGE =
-      TILE_C + (UPD ? TILE_C + (RADIAL ? 0 : 2 * TILE_R + (CHI ? TILE_R : 0)) : 0);
+      TILE_C + (UPD ? TILE_C + (OPS != 0 ? 0 : 2 * TILE_R + (CHI ? TILE_R : 0)) : 0);
   static constexpr size_t TW = align128(size_t(N) * sizeof(C));
   static constexpr int S0 = int((kMaxDynSmem - TW - 128) / STAGE);
   static constexpr int STAGES = S0 > 3 ? 3 : S0;
@@ -109,15 +110,16 @@ __device__ __forceinline__ void radial_ops(const ColArgs<Real> &a, int kx, int k
 
 // Tensor maps: PLAIN uses m0 (array set 0) and m1 (array set 1); UPDATE uses
 // m0 = N_hat partial (A), m1 = psi_hat, m2 = tab_a, m3 = tab_b, m4 = tab_chi
-// (m2..m4 unused with RADIAL).
-template <typename Real, int N, int W, int MODE, int DIR, int MODEL, bool INV, bool RADIAL>
-__global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
+// (m2..m4 unused unless OPS == 0, per-mode tables).  MINB CTAs share an SM.
+template <typename Real, int N, int W, int MODE, int DIR, int MODEL, bool INV, int OPS, int MINB>
+__global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
     col_tma_kernel(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
                    const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3,
                    const __grid_constant__ CUtensorMap m4, const ColArgs<Real> a, const int axis,
                    unsigned *flag) {
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, RADIAL>;
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS>;
   using C = typename Cx<Real>::T;
+  constexpr bool RADIAL = OPS == 1;
   constexpr int E = Plan<N>::E;
   constexpr int T = N / E;
   constexpr int NT = W * T;
@@ -158,7 +160,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
       if constexpr (UPD) {
         const size_t offr = size_t(b) * Cfg::RB * W * sizeof(Real);
         tma_load_3d(st + Cfg::TILE_C + offc, &m1, &bars[s], ti * W * 2, y, z);
-        if constexpr (RADIAL) continue;
+        if constexpr (OPS != 0) continue;
         tma_load_3d(st + 2 * Cfg::TILE_C + offr, &m2, &bars[s], ti * W, y, z);
         tma_load_3d(st + 2 * Cfg::TILE_C + Cfg::TILE_R + offr, &m3, &bars[s], ti * W, y, z);
         if constexpr (Cfg::CHI)
@@ -228,6 +230,8 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
           la = rla[m];
           lb = rlb[m];
           if constexpr (Cfg::CHI) ch = rch[m];
+        } else if constexpr (OPS == 2) {
+          computed_ops<Real, MODEL>(a, ti * W + c, to, j + T * m, la, lb, ch);
         } else {
           la = ta[e];
           lb = tb[e];
@@ -308,6 +312,8 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), 1)
           Real la, lb;
           if constexpr (RADIAL) {
             radial_ops(a, a.rad_M, cg, j + T * m, la, lb, ch);  // Nyquist plane: kx = M, ky = column
+          } else if constexpr (OPS == 2) {
+            computed_ops<Real, MODEL>(a, a.rad_M, cg, j + T * m, la, lb, ch);
           } else {
             la = a.tab_a[idx];
             lb = a.tab_b[idx];

@@ -36,6 +36,28 @@ template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
 }
 template <typename C> __device__ __forceinline__ C cscale(C a, decltype(C::x) s) { return mk<C>(a.x * s, a.y * s); }
 
+// pf2: FP32 complex whose add / subtract / real scale issue as one packed
+// FP32x2 instruction (sm_100) instead of two scalar ones.  Each lane is rounded
+// exactly as the scalar operation (a - b is fma(b, -1, a): one rounding of the
+// exact difference), so results are bit-identical to float2 arithmetic.  Kernels
+// opt in through CxP (the x passes, where it measured faster; the column passes
+// stay on float2, where it did not).
+struct __align__(8) pf2 {
+  float x, y;
+};
+template <typename R> struct CxP { using T = typename Cx<R>::T; };
+template <> struct CxP<float> { using T = pf2; };
+
+__device__ __forceinline__ float2 f2(pf2 a) { return make_float2(a.x, a.y); }
+__device__ __forceinline__ pf2 p2(float2 a) { return pf2{a.x, a.y}; }
+template <> __device__ __forceinline__ pf2 cadd<pf2>(pf2 a, pf2 b) { return p2(__fadd2_rn(f2(a), f2(b))); }
+template <> __device__ __forceinline__ pf2 csub<pf2>(pf2 a, pf2 b) {
+  return p2(__ffma2_rn(f2(b), make_float2(-1.f, -1.f), f2(a)));
+}
+template <> __device__ __forceinline__ pf2 cscale<pf2>(pf2 a, float s) {
+  return p2(__fmul2_rn(f2(a), make_float2(s, s)));
+}
+
 // a * w (DIR < 0) or a * conj(w) (DIR > 0)
 template <int DIR, typename C> __device__ __forceinline__ C twmul(C a, C w) {
   if (DIR < 0) return mk<C>(a.x * w.x - a.y * w.y, a.x * w.y + a.y * w.x);

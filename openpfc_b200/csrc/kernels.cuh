@@ -35,7 +35,34 @@ template <typename Real> struct ColArgs {
   const void *rad_ops;
   const Real *rad_chi;
   int rad_M, rad_n1, rad_n2;
+  // computed operators: wavenumber steps, r, dt, 1/(2 alpha^2)
+  Real kf0, kf1, kf2, op_r, op_dt, op_chi;
 };
+
+// Operator selection of the fused z update.
+enum OpsKind { OPS_TABLES = 0, OPS_RADIAL = 1, OPS_COMPUTED = 2 };
+
+// Plain-PFC operators of mode (kx, ky, kz) (kx unfolded, ky / kz folded), in
+// the compute precision (10_complete_pfc_model.cpp:189-207, kspace.hpp:97-103):
+//   k^2 = sum (f_a i_a)^2, g = r + (1 - k^2)^2, L = -k^2 g,
+//   opL = exp(L dt),  opN = (opL - 1)/L (-k^2) = expm1(L dt)/g  (|L| > 1e-14),
+//   opN = dt (-k^2) otherwise;  FILTERED: chi = exp(-k^2 / (2 alpha^2)).
+// expm1 keeps the long-wavelength modes (|L dt| << 1) accurate in FP32.
+template <typename Real, int MODEL>
+__device__ __forceinline__ void computed_ops(const ColArgs<Real> &a, int kx, int ky, int kz, Real &la,
+                                             Real &lb, Real &ch) {
+  const int fy = ky <= a.rad_n1 / 2 ? ky : a.rad_n1 - ky;
+  const int fz = kz <= a.rad_n2 / 2 ? kz : a.rad_n2 - kz;
+  const Real qx = a.kf0 * Real(kx), qy = a.kf1 * Real(fy), qz = a.kf2 * Real(fz);
+  const Real k2 = qx * qx + qy * qy + qz * qz;
+  const Real u = Real(1) - k2;
+  const Real g = a.op_r + u * u;
+  const Real L = -k2 * g;
+  const Real x = L * a.op_dt;
+  la = exp(x);
+  lb = fabs(L) > Real(1e-14) ? expm1(x) / g : -a.op_dt * k2;
+  ch = MODEL == MK_FILTERED ? exp(-k2 * a.op_chi) : Real(1);
+}
 
 template <typename C> __device__ __forceinline__ C czero() { return mk<C>(0, 0); }
 }  // namespace opfc
@@ -47,7 +74,7 @@ namespace opfc {
 // ---------------------------------------------------------------------------
 // column pass: batched FFT along a strided axis (y or z), optional ETD update
 // ---------------------------------------------------------------------------
-template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS>
 __global__ void __launch_bounds__(Width<Real>::W *(N / Plan<N>::E))
     col_kernel(const ColArgs<Real> a) {
   using C = typename Cx<Real>::T;
@@ -101,14 +128,18 @@ __global__ void __launch_bounds__(Width<Real>::W *(N / Plan<N>::E))
       C np = czero<C>();
       if (ok) {
         const C p = ph[idx];
-        const Real la = a.tab_a[idx];
-        const Real lb = a.tab_b[idx];
+        Real la, lb, ch = Real(1);
+        if constexpr (OPS == OPS_COMPUTED) {
+          // z pass: main plane kx = column, ky = outer; Nyquist plane kx = M, ky = column
+          computed_ops<Real, MODEL>(a, second ? a.rad_M : cg, second ? cg : to, j + T * m, la, lb, ch);
+        } else {
+          la = a.tab_a[idx];
+          lb = a.tab_b[idx];
+          if constexpr (MODEL != MK_PLAIN) ch = a.tab_chi[idx];
+        }
         np = mk<C>(la * p.x + lb * v[m].x, la * p.y + lb * v[m].y);
         ph[idx] = np;
-        if constexpr (MODEL != MK_PLAIN) {
-          const Real ch = a.tab_chi[idx];
-          w[m] = cscale(np, ch);
-        }
+        if constexpr (MODEL != MK_PLAIN) w[m] = cscale(np, ch);
       } else if constexpr (MODEL != MK_PLAIN) {
         w[m] = czero<C>();
       }
@@ -517,72 +548,7 @@ static inline ColSeg retile(ColSeg g, int W, int Wold) {
   return g;
 }
 
-template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, bool RADIAL>
-static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
-  using C = typename Cx<Real>::T;
-  constexpr int W = tma_col_width(N, (int)sizeof(C), MODE);
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, RADIAL>;
-  if constexpr (Cfg::STAGES < 1) {
-    return -1;
-  } else {
-    if (L.seg[0].ncols % W != 0 || L.seg[0].col_stride != 1) return -1;
-    constexpr int NT = W * (N / Plan<N>::E);
-    auto k = col_tma_kernel<Real, N, W, MODE, DIR, MODEL, INV, RADIAL>;
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-      attr = true;
-    }
-    ColArgs<Real> a;
-    a.seg0 = retile(L.seg[0], W, Width<Real>::W);
-    a.seg1 = L.nseg < 2 ? ColSeg{} : retile(L.seg[1], W, Width<Real>::W);
-    a.in[0] = L.in[0];
-    a.in[1] = L.in[1];
-    a.out[0] = L.out[0];
-    a.out[1] = L.out[1];
-    a.tw = L.tw;
-    a.psi_hat = L.psi_hat;
-    a.tab_a = reinterpret_cast<const Real *>(L.tab_a);
-    a.tab_b = reinterpret_cast<const Real *>(L.tab_b);
-    a.tab_chi = reinterpret_cast<const Real *>(L.tab_chi);
-    a.rad_ops = L.rad_ops;
-    a.rad_chi = reinterpret_cast<const Real *>(L.rad_chi);
-    a.rad_M = L.rad_M;
-    a.rad_n1 = L.rad_n1;
-    a.rad_n2 = L.rad_n2;
-    const CUtensorMap *t0 = reinterpret_cast<const CUtensorMap *>(L.tmap[0]);
-    auto pick = [&](int i) { return L.tmap[i] ? *reinterpret_cast<const CUtensorMap *>(L.tmap[i]) : *t0; };
-    int G = L.num_sms > 0 ? L.num_sms : 148;
-    const int most = a.seg0.ntiles > a.seg1.ntiles ? a.seg0.ntiles : a.seg1.ntiles;
-    if (G > most) G = most;
-    if (G < 1) return 0;
-    dim3 grid(G, MODE == COL_PLAIN ? L.nsets : 1);
-    k<<<grid, NT, Cfg::SMEM, s>>>(*t0, pick(1), pick(2), pick(3), pick(4), a, L.axis, L.flag);
-    return (int)cudaGetLastError();
-  }
-}
-
-template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
-static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
-  using C = typename Cx<Real>::T;
-  if (L.tmap[0]) {
-    int rc;
-    if constexpr (MODE == COL_UPDATE)
-      rc = L.rad_ops ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, true>(L, s)
-                     : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, false>(L, s);
-    else
-      rc = launch_col_tma<Real, N, MODE, DIR, MODEL, INV, false>(L, s);
-    if (rc >= 0) return rc;
-  }
-  constexpr int W = Width<Real>::W;
-  constexpr int NT = W * (N / Plan<N>::E);
-  const size_t smem = sizeof(C) * ((size_t)N + (size_t)N * (W + 1));
-  auto k = col_kernel<Real, N, MODE, DIR, MODEL, INV>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+template <typename Real> static ColArgs<Real> col_args(const ColLaunch &L) {
   ColArgs<Real> a;
   a.seg0 = L.seg[0];
   a.seg1 = L.seg[1];
@@ -596,11 +562,94 @@ static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
   a.tab_a = reinterpret_cast<const Real *>(L.tab_a);
   a.tab_b = reinterpret_cast<const Real *>(L.tab_b);
   a.tab_chi = reinterpret_cast<const Real *>(L.tab_chi);
+  a.rad_ops = L.rad_ops;
+  a.rad_chi = reinterpret_cast<const Real *>(L.rad_chi);
+  a.rad_M = L.rad_M;
+  a.rad_n1 = L.rad_n1;
+  a.rad_n2 = L.rad_n2;
+  a.kf0 = (Real)L.kf[0];
+  a.kf1 = (Real)L.kf[1];
+  a.kf2 = (Real)L.kf[2];
+  a.op_r = (Real)L.op_r;
+  a.op_dt = (Real)L.op_dt;
+  a.op_chi = (Real)L.op_chi;
+  return a;
+}
+
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS>
+static int launch_col_direct(const ColLaunch &L, cudaStream_t s) {
+  using C = typename Cx<Real>::T;
+  constexpr int W = Width<Real>::W;
+  constexpr int NT = W * (N / Plan<N>::E);
+  const size_t smem = sizeof(C) * ((size_t)N + (size_t)N * (W + 1));
+  auto k = col_kernel<Real, N, MODE, DIR, MODEL, INV, OPS>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    attr = true;
+  }
+  ColArgs<Real> a = col_args<Real>(L);
   const int tiles = a.seg0.ntiles + a.seg1.ntiles;
   if (tiles == 0) return 0;
   dim3 grid(tiles, MODE == COL_PLAIN ? L.nsets : 1);
   k<<<grid, NT, smem, s>>>(a);
   return (int)cudaGetLastError();
+}
+
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS, bool NARROW>
+static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
+  using C = typename Cx<Real>::T;
+  constexpr int W = tma_col_width(N, (int)sizeof(C), MODE, NARROW);
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS>;
+  constexpr int NT = W * (N / Plan<N>::E);
+  // narrow tiles: two CTAs per SM when their shared memory fits and each has at
+  // most 512 threads (64 registers per thread)
+  constexpr int MINB = (NARROW && 2 * (Cfg::SMEM + 1024) <= 233472 && NT <= 512) ? 2 : 1;
+  if constexpr (Cfg::STAGES < 1 || (NARROW && MINB < 2) ||
+                (OPS == OPS_COMPUTED && MODEL == MK_TUNGSTEN)) {
+    return -1;
+  } else {
+    if (L.seg[0].ncols % W != 0 || L.seg[0].col_stride != 1) return -1;
+    auto k = col_tma_kernel<Real, N, W, MODE, DIR, MODEL, INV, OPS, MINB>;
+    static int occ = 0;
+    if (!occ) {
+      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, NT, Cfg::SMEM) != cudaSuccess || occ < 1)
+        occ = 1;
+      if (occ > MINB) occ = MINB;
+    }
+    ColArgs<Real> a = col_args<Real>(L);
+    a.seg0 = retile(L.seg[0], W, Width<Real>::W);
+    a.seg1 = L.nseg < 2 ? ColSeg{} : retile(L.seg[1], W, Width<Real>::W);
+    const CUtensorMap *t0 = reinterpret_cast<const CUtensorMap *>(L.tmap[0]);
+    auto pick = [&](int i) { return L.tmap[i] ? *reinterpret_cast<const CUtensorMap *>(L.tmap[i]) : *t0; };
+    int G = (L.num_sms > 0 ? L.num_sms : 148) * occ;
+    const int most = a.seg0.ntiles > a.seg1.ntiles ? a.seg0.ntiles : a.seg1.ntiles;
+    if (G > most) G = most;
+    if (G < 1) return 0;
+    dim3 grid(G, MODE == COL_PLAIN ? L.nsets : 1);
+    k<<<grid, NT, Cfg::SMEM, s>>>(*t0, pick(1), pick(2), pick(3), pick(4), a, L.axis, L.flag);
+    return (int)cudaGetLastError();
+  }
+}
+
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
+static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
+  if (L.tmap[0]) {
+    int rc;
+    if constexpr (MODE == COL_UPDATE)
+      rc = L.rad_ops    ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_RADIAL, false>(L, s)
+           : L.computed ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false>(L, s)
+                        : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false>(L, s);
+    else
+      rc = L.narrow ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, true>(L, s)
+                    : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false>(L, s);
+    if (rc >= 0) return rc;
+  }
+  if constexpr (MODE == COL_UPDATE && MODEL != MK_TUNGSTEN) {
+    if (L.computed) return launch_col_direct<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED>(L, s);
+  }
+  return launch_col_direct<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES>(L, s);
 }
 
 template <typename Real, int N>

@@ -58,18 +58,25 @@ struct ColLaunch {
   const void *rad_ops;
   const void *rad_chi;
   int rad_M, rad_n1, rad_n2;
+  // COL_UPDATE, PLAIN and FILTERED models: operators computed per mode from k^2
+  // in the compute precision (no table is read); kf = 2 pi / (dx n) per axis,
+  // op_chi = 1 / (2 alpha^2) of the filter (FILTERED).  Uses rad_M/n1/n2.
+  int computed;
+  double kf[3], op_r, op_dt, op_chi;
+  // COL_PLAIN: half-width tiles (64-byte rows) with two CTAs per SM
+  int narrow;
   int axis;            // 1 = y, 2 = z
   unsigned int *flag;  // bit 1: a bounded wait expired
   int num_sms;
 };
 
 // Tile width (columns) of the TMA column kernels: 128-byte rows for the plain
-// transforms and 64-byte rows for the fused update (which stages psi_hat and the
-// tables too), capped so one tile stays near 64 KB / 32 KB.  Host and device
-// use this one definition.
-constexpr int tma_col_width(int N, int csize, int mode) {
-  int w = (mode == COL_PLAIN ? 128 : 64) / csize;
-  const int cap = (mode == COL_PLAIN ? 65536 : 32768) / (N * csize);
+// transforms (64-byte rows and half the tile for the narrow variant) and 64-byte
+// rows for the fused update (which stages psi_hat and the tables too), capped so
+// one tile stays near 64 KB / 32 KB.  Host and device use this one definition.
+constexpr int tma_col_width(int N, int csize, int mode, bool narrow = false) {
+  int w = (mode == COL_PLAIN && !narrow ? 128 : 64) / csize;
+  const int cap = (mode == COL_PLAIN && !narrow ? 65536 : 32768) / (N * csize);
   if (cap < w) w = cap;
   return w < 4 ? 4 : w;
 }

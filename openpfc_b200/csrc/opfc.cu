@@ -36,6 +36,7 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
+constexpr int kVarY = 3, kVarX = 2, kVarZ = 5;  // kernel variants per pass (opfc_autotune)
 
 bool supported_len(int n) {
   static const int ok[] = {1, 2, 4, 8, 16, 24, 32, 40, 48, 64, 80, 96, 128, 256, 512, 1024};
@@ -125,8 +126,11 @@ struct opfc_handle {
 
   bool use_tma = true;  // TMA-fed column passes (OPFC_NO_TMA=1 disables)
   // kernel variants per pass, chosen by the autotuner (see opfc_autotune):
-  // var_y: 0 pipelined, 1 direct; var_x: 0 pipelined, 1 direct;
-  // var_z: 0 pipelined with streamed tables, 1 pipelined with radial tables, 2 direct
+  // var_y: 0 pipelined, 1 direct, 2 pipelined narrow tiles (two CTAs per SM);
+  // var_x: 0 pipelined, 1 direct;
+  // var_z: 0 pipelined with streamed tables, 1 pipelined with radial tables,
+  //        2 direct with streamed tables, 3 pipelined with computed operators,
+  //        4 direct with computed operators (3, 4: PLAIN and FILTERED)
   int var_y = 0, var_x = 0, var_z = 0;
   int num_sms = 148;
   struct Tmap {
@@ -292,8 +296,9 @@ int col_plain(opfc_handle *h, int axis, int dir, const void *in0, void *out0,
   L.out[1] = out1 ? out1 : out0;
   L.tw = axis == 1 ? h->tw_y : h->tw_z;
   L.axis = axis;
-  const int W = tma_col_width(L.N, 2 * (int)h->rsz, COL_PLAIN);
-  if (h->use_tma && h->var_y == 0 && L.N > 1 && h->M % W == 0) {
+  L.narrow = h->var_y == 2;
+  const int W = tma_col_width(L.N, 2 * (int)h->rsz, COL_PLAIN, L.narrow);
+  if (h->use_tma && h->var_y != 1 && L.N > 1 && h->M % W == 0) {
     L.tmap[0] = tmap_for(h, in0, axis, W, false);
     L.tmap[1] = in1 ? tmap_for(h, in1, axis, W, false) : nullptr;
     if (in1 && !L.tmap[1]) L.tmap[0] = nullptr;
@@ -455,11 +460,23 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.tab_b = h->tab_b;
     Z.tab_chi = h->tab_chi;
     Z.axis = 2;
+    // computed operators (variants 3, 4): PLAIN and FILTERED models
+    Z.computed = (h->var_z == 3 || h->var_z == 4) && model != OPFC_MODEL_TUNGSTEN;
+    Z.rad_M = h->M;
+    Z.rad_n1 = h->n1;
+    Z.rad_n2 = h->n2;
+    const int nn[3] = {h->n0, h->n1, h->n2};
+    for (int a = 0; a < 3; ++a) Z.kf[a] = 2.0 * kPi / (h->desc.dx[a] * nn[a]);
+    Z.op_r = h->desc.r;
+    Z.op_dt = h->dt;
+    Z.op_chi = model == OPFC_MODEL_FILTERED ? 1.0 / (2.0 * h->desc.filter_alpha * h->desc.filter_alpha) : 0.0;
     const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE);
-    if (h->use_tma && h->var_z != 2 && Z.N > 1 && h->M % W == 0) {
+    if (h->use_tma && h->var_z != 2 && h->var_z != 4 && Z.N > 1 && h->M % W == 0) {
       Z.tmap[0] = tmap_for(h, h->work_a, 2, W, false);
       Z.tmap[1] = tmap_for(h, h->psi_hat, 2, W, false);
-      if (h->rad_ops && h->var_z == 1) {
+      if (Z.computed) {
+        if (!Z.tmap[1]) Z.tmap[0] = nullptr;
+      } else if (h->rad_ops && h->var_z == 1) {
         // isotropic grid: operators from the L2-resident radial tables
         Z.rad_ops = h->rad_ops;
         Z.rad_chi = h->rad_chi;
@@ -949,12 +966,16 @@ int opfc_initialize(opfc_handle *h, double dt) {
   }
   h->dt = dt;
   // kernel variants: the autotuner's cached choice, else the defaults;
-  // OPFC_Z_VARIANT forces the z-update variant (0 tables, 1 radial, 2 direct)
+  // OPFC_Z_VARIANT / OPFC_Y_VARIANT force the z-update / y-pass variant
   h->var_y = AutoTuner::instance().get_config(tune_key(h, "y"), 0);
   h->var_x = AutoTuner::instance().get_config(tune_key(h, "x"), 0);
   h->var_z = AutoTuner::instance().get_config(tune_key(h, "z"), 0);
   if (const char *zv = std::getenv("OPFC_Z_VARIANT")) h->var_z = std::atoi(zv);
+  if (const char *yv = std::getenv("OPFC_Y_VARIANT")) h->var_y = std::atoi(yv);
   if (h->var_z == 1 && !h->rad_ops) h->var_z = 0;
+  if (h->var_z >= 3 && model == OPFC_MODEL_TUNGSTEN) h->var_z = h->var_z == 4 ? 2 : 0;
+  if (h->var_z < 0 || h->var_z >= kVarZ) h->var_z = 0;
+  if (h->var_y < 0 || h->var_y >= kVarY) h->var_y = 0;
   h->initialized = true;
   h->a_valid = false;
   release_graph(h);
@@ -1172,12 +1193,13 @@ int opfc_autotune(opfc_handle *h, double *ms) {
   AutoTuner &T = AutoTuner::instance();
   std::vector<double> my, mx, mz;
   // each candidate runs its pass alone, in place on whatever the arrays hold
-  h->var_y = T.tune(tune_key(h, "y"), 2, [&](int v) { h->var_y = v; return enqueue_step(h, 0); }, h->stream, &my);
-  h->var_x = T.tune(tune_key(h, "x"), 2, [&](int v) { h->var_x = v; return enqueue_step(h, 1); }, h->stream, &mx);
+  h->var_y = T.tune(tune_key(h, "y"), kVarY, [&](int v) { h->var_y = v; return enqueue_step(h, 0); }, h->stream, &my);
+  h->var_x = T.tune(tune_key(h, "x"), kVarX, [&](int v) { h->var_x = v; return enqueue_step(h, 1); }, h->stream, &mx);
   h->var_z = T.tune(
-      tune_key(h, "z"), 3,
+      tune_key(h, "z"), kVarZ,
       [&](int v) {
         if (v == 1 && !h->rad_ops) return (int)OPFC_ERR_ARG;
+        if (v >= 3 && h->desc.model == OPFC_MODEL_TUNGSTEN) return (int)OPFC_ERR_ARG;
         h->var_z = v;
         return enqueue_step(h, 3);
       },
@@ -1188,9 +1210,10 @@ int opfc_autotune(opfc_handle *h, double *ms) {
   h->a_valid = false;
   if (ms) {
     const std::vector<double> *all[3] = {&my, &mx, &mz};
+    const int cnt[3] = {kVarY, kVarX, kVarZ};
     int o = 0;
     for (int p = 0; p < 3; ++p)
-      for (int v = 0; v < (p == 2 ? 3 : 2); ++v) ms[o++] = (int)all[p]->size() > v ? (*all[p])[v] : -1.0;
+      for (int v = 0; v < cnt[p]; ++v) ms[o++] = (int)all[p]->size() > v ? (*all[p])[v] : -1.0;
   }
   return OPFC_OK;
 }

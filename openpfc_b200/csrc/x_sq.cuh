@@ -15,7 +15,7 @@
 namespace opfc {
 
 template <typename Real, int R, int MODEL> struct XSqCfg {
-  using C = typename Cx<Real>::T;
+  using C = typename CxP<Real>::T;
   static constexpr int M = R * R;
   static constexpr int W = Width<Real>::W;  // rows (lines) per tile
   static constexpr int P = M + 2;           // padded row pitch of the landed tile
@@ -59,7 +59,7 @@ __device__ __forceinline__ void fft_sq(C (&v)[R], C *ex, int j, const C *tws) {
 template <typename Real, int R, int MODEL>
 __global__ void __launch_bounds__(Width<Real>::W *R) x_sq_kernel(const XArgs<Real> a) {
   using Cfg = XSqCfg<Real, R, MODEL>;
-  using C = typename Cx<Real>::T;
+  using C = typename CxP<Real>::T;
   constexpr int M = Cfg::M;
   constexpr int W = Cfg::W;
   constexpr int NT = W * R;

@@ -22,7 +22,7 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, unsigned b
 }
 
 template <typename Real, int M, int MODEL> struct XCfg {
-  using C = typename Cx<Real>::T;
+  using C = typename CxP<Real>::T;
   static constexpr int W = Width<Real>::W;
   static constexpr int P = M + 2;  // padded row pitch in complex values (16-byte multiple)
   static constexpr size_t TILE = size_t(W) * P * sizeof(C) + size_t(W) * sizeof(C);
@@ -61,7 +61,7 @@ template <typename Real, int M, int MODEL>
 __global__ void __launch_bounds__(Width<Real>::W *(M / Plan<M>::E))
     x_tma_kernel(const XArgs<Real> a) {
   using Cfg = XCfg<Real, M, MODEL>;
-  using C = typename Cx<Real>::T;
+  using C = typename CxP<Real>::T;
   constexpr int W = Cfg::W;
   constexpr int E = Plan<M>::E;
   constexpr int T = M / E;

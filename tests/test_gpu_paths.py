@@ -14,19 +14,29 @@ pytestmark = pytest.mark.gpu
 PI4 = [math.pi / 4] * 3
 
 
-@pytest.fixture(params=["tma", "tma_radial", "direct"])
+@pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed"])
 def path(request, monkeypatch):
     """tma: pipelined kernels streaming the per-mode tables (default);
     tma_radial: the z update reading radial operator tables (OPFC_Z_VARIANT=1,
     isotropic grids; others fall back to tables);
-    direct: direct-load kernels (OPFC_NO_TMA=1)."""
+    direct: direct-load kernels (OPFC_NO_TMA=1);
+    computed: pipelined z update computing its operators from k^2
+    (OPFC_Z_VARIANT=3) and half-width y tiles (OPFC_Y_VARIANT=2);
+    direct_computed: direct z update computing its operators (OPFC_Z_VARIANT=4).
+    The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
+    monkeypatch.delenv("OPFC_Y_VARIANT", raising=False)
     monkeypatch.setenv("OPENPFC_GPU_AUTOTUNE_MODE", "fallback_only")
     if request.param == "direct":
         monkeypatch.setenv("OPFC_NO_TMA", "1")
     elif request.param == "tma_radial":
         monkeypatch.setenv("OPFC_Z_VARIANT", "1")
+    elif request.param == "computed":
+        monkeypatch.setenv("OPFC_Z_VARIANT", "3")
+        monkeypatch.setenv("OPFC_Y_VARIANT", "2")
+    elif request.param == "direct_computed":
+        monkeypatch.setenv("OPFC_Z_VARIANT", "4")
     return request.param
 
 
@@ -89,7 +99,8 @@ def test_autotune_then_parity(oracle, tmp_path, monkeypatch):
     m = ob.PfcB200(n, PI4, precision=ob.FP32)
     m.initialize(0.5)
     ms = m.autotune()
-    assert ms["y.pipelined"] > 0 and ms["z.tables"] > 0 and ms["z.radial"] > 0
+    assert ms["y.pipelined"] > 0 and ms["y.narrow"] > 0 and ms["z.tables"] > 0 and ms["z.radial"] > 0
+    assert ms["z.computed"] > 0 and ms["z.direct_computed"] > 0
     chosen = m.variants()
     m.set_psi(psi0)
     m.step(10)
