@@ -120,12 +120,21 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def alg_bytes_per_kernel(n, prec_bytes):
-    """Algorithmic HBM bytes per launch of each kernel of the plain step."""
+def z_tables(var_z, t):
+    """Per-mode operator tables the z-update variant streams from HBM: t for the
+    table variants (0, 2), none when the operators come from the L2-resident
+    radial table (1) or are computed from k^2 (3, 4)."""
+    return t if var_z in (0, 2) else 0
+
+
+def alg_bytes_per_kernel(n, prec_bytes, tables=2):
+    """Algorithmic HBM bytes per launch of each kernel of the plain step: every
+    pass reads and writes each complex mode once; the z update also reads and
+    writes psi_hat and reads `tables` per-mode operator tables."""
     nc = (n // 2 + 1) * n * n
     sc, st = 2 * prec_bytes, prec_bytes
     return {"y_inverse": 2 * nc * sc, "x_fused": 2 * nc * sc, "y_forward": 2 * nc * sc,
-            "z_update": nc * (4 * sc + 2 * st), "hermitian_fix": 4 * 2 * n * n * sc}
+            "z_update": nc * (4 * sc + tables * st), "hermitian_fix": 4 * 2 * n * n * sc}
 
 
 def cpu_baseline(psi0, budget_s=30.0):
@@ -211,7 +220,9 @@ def run_b200(args):
 
     m = ob.PfcB200((N, N, N), DX, r=R, precision=ob.FP32, device=local)
     m.initialize(DT)
-    tune32 = m.autotune()  # kernel variant per pass, timed on this GPU (untimed set-up)
+    # kernel variant per pass, timed on this GPU (untimed set-up); --no-autotune
+    # keeps the cached or default choice (OPFC_Y_VARIANT / OPFC_Z_VARIANT force one)
+    tune32 = None if args.no_autotune else m.autotune()
     m.set_psi(psi0_32)
     stream = torch.cuda.ExternalStream(m.stream, device=torch.device("cuda", local))
     # clocks are sampled from the warm-up through the end of the timed region
@@ -280,7 +291,7 @@ def run_b200(args):
     # per-kernel device time (each kernel alone, CUDA events on the handle's stream)
     m.set_psi(psi0_32)
     prof = m.profile_step(reps=args.profile_reps)
-    ab = alg_bytes_per_kernel(N, 4)
+    ab = alg_bytes_per_kernel(N, 4, z_tables(m.variants()[2], 2))
     passes = {}
     for k, t in prof.items():
         gbs = ab[k] / (t / 1e3) / 1e9
@@ -290,7 +301,11 @@ def run_b200(args):
     tpath = os.path.join(ROOT, "profiles", "traffic_512.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(dom)
+            # per-launch DRAM bytes from ncu, keyed "<pass>/v<variant>" (the
+            # variant of that pass this run uses)
+            var = {"y_inverse": m.variants()[0], "y_forward": m.variants()[0], "x_fused": m.variants()[1],
+                   "z_update": m.variants()[2]}.get(dom, 0)
+            traffic = json.load(open(tpath)).get(f"{dom}/v{var}")
         except Exception:
             traffic = None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": passes[dom]["gbs"], "peak": hbm,
@@ -334,7 +349,7 @@ def run_filtered(args):
     t_ic = time.time() - t0
     m = ob.FilteredB200((n, n, n), DX, r=-0.3, alpha=0.5, p2=-0.1, p3=-0.5, p4=0.3, precision=ob.FP32)
     m.initialize(DT)
-    tune = m.autotune()
+    tune = None if args.no_autotune else m.autotune()
     m.set_psi(psi0)
     del psi0
     stream = torch.cuda.ExternalStream(m.stream)
@@ -343,8 +358,8 @@ def run_filtered(args):
     cells = n ** 3
     nc = (n // 2 + 1) * n * n
     prof = m.profile_step(reps=max(2, args.profile_reps // 2))
-    ab = {"y_inverse": 16 * nc, "x_fused": 16 * nc, "y_forward": 16 * nc, "z_update": nc * (32 + 12),
-          "hermitian_fix": 4 * 2 * n * n * 8}
+    ab = {"y_inverse": 16 * nc, "x_fused": 16 * nc, "y_forward": 16 * nc,
+          "z_update": nc * (32 + 4 * z_tables(m.variants()[2], 3)), "hermitian_fix": 4 * 2 * n * n * 8}
     passes = {k: {"ms": t, "gbs": ab[k] / (t / 1e3) / 1e9, "frac": ab[k] / (t / 1e3) / 1e9 / hbm}
               for k, t in prof.items()}
     line = {"metric": "Mcell-steps/s, filtered PFC 1024^3 FP32", "value": cells * args.steps / (ms / 1e3) / 1e6,
@@ -424,6 +439,8 @@ def main(argv=None):
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-reps", type=int, default=10)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the cached (or default) kernel variants instead of timing them first")
     ap.add_argument("--workload", default="plain", choices=["plain", "filtered", "ensemble"],
                     help="plain: the measured 512^3 line; filtered: mean-field-filtered 1024^3 FP32; "
                          "ensemble: 256 uneven members, 50 steps in one graph")

@@ -76,7 +76,7 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 constexpr int kMaxDynSmem = 232448;  // 227 KB opt-in per CTA on sm_100
 
-template <typename Real, int N, int W, int MODE, int MODEL, int OPS = 0> struct TmaCfg {
+template <typename Real, int N, int W, int MODE, int MODEL, int OPS = 0, int SCAP = 3> struct TmaCfg {
   using C = typename Cx<Real>::T;
   static constexpr bool UPD = MODE == COL_UPDATE;
   static constexpr bool CHI = UPD && MODEL != MK_PLAIN;
@@ -84,11 +84,12 @@ template <typename Real, int N, int W, int MODE, int MODEL, int OPS = 0> struct 
   static constexpr size_t TILE_R = size_t(N) * W * sizeof(Real);
   // radial operators come from an L2-resident table and computed operators
   // from k^2: only the per-mode tables are staged
+  // (OPS 3: psi_hat is not staged either)
   static constexpr size_t STAGE =
-      TILE_C + (UPD ? TILE_C + (OPS != 0 ? 0 : 2 * TILE_R + (CHI ? TILE_R : 0)) : 0);
+      TILE_C + (UPD ? (OPS == 3 ? 0 : TILE_C) + (OPS != 0 ? 0 : 2 * TILE_R + (CHI ? TILE_R : 0)) : 0);
   static constexpr size_t TW = align128(size_t(N) * sizeof(C));
   static constexpr int S0 = int((kMaxDynSmem - TW - 128) / STAGE);
-  static constexpr int STAGES = S0 > 3 ? 3 : S0;
+  static constexpr int STAGES = S0 > SCAP ? SCAP : S0;
   static constexpr size_t SMEM = TW + size_t(STAGES > 0 ? STAGES : 1) * STAGE + 64;
   static constexpr int RB = N < 256 ? N : 256;  // rows per TMA box (box dims <= 256)
   static constexpr int NB = N / RB;
@@ -108,6 +109,17 @@ __device__ __forceinline__ void radial_ops(const ColArgs<Real> &a, int kx, int k
   ch = a.rad_chi ? __ldg(a.rad_chi + m) : Real(1);
 }
 
+// Update-mode transform: stage twiddles from the register cache (TWR) or the
+// shared table.
+template <typename C, int N, int D, bool TWR>
+__device__ __forceinline__ void upd_fft(C (&x)[Plan<N>::E], C *buf, int ld, int c, int j, const C *tw,
+                                        const TwReg<C, N> &twr) {
+  if constexpr (TWR)
+    fft_line_rt<C, N, D>(x, buf, ld, c, j, twr);
+  else
+    fft_line<C, N, D, N>(x, buf, ld, c, j, tw);
+}
+
 // Tensor maps: PLAIN uses m0 (array set 0) and m1 (array set 1); UPDATE uses
 // m0 = N_hat partial (A), m1 = psi_hat, m2 = tab_a, m3 = tab_b, m4 = tab_chi
 // (m2..m4 unused unless OPS == 0, per-mode tables).  MINB CTAs share an SM.
@@ -117,9 +129,12 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
                    const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3,
                    const __grid_constant__ CUtensorMap m4, const ColArgs<Real> a, const int axis,
                    unsigned *flag) {
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS>;
+  // two CTAs per SM for the update: one stage each
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, (MINB > 1 && MODE == COL_UPDATE) ? 1 : 3>;
   using C = typename Cx<Real>::T;
   constexpr bool RADIAL = OPS == 1;
+  constexpr bool COMPUTED = OPS == 2 || OPS == 3;
+  constexpr bool PD = OPS == 3;  // psi_hat straight into registers
   constexpr int E = Plan<N>::E;
   constexpr int T = N / E;
   constexpr int NT = W * T;
@@ -140,6 +155,11 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
     mbar_fence_init();
   }
   __syncthreads();
+  // the update's two transforms per tile take their stage twiddles from
+  // registers when few enough (loaded once: they depend only on j)
+  constexpr bool TWR = UPD && MINB == 1 && TwReg<C, N>::CNT > 0 && TwReg<C, N>::CNT <= 16;
+  TwReg<C, N> twr;
+  if constexpr (TWR) twr.load(j, tw);
 
   const int set = blockIdx.y;
   const CUtensorMap *min = (MODE == COL_PLAIN && set == 1) ? &m1 : &m0;
@@ -159,7 +179,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
       tma_load_3d(st + offc, min, &bars[s], ti * W * 2, y, z);
       if constexpr (UPD) {
         const size_t offr = size_t(b) * Cfg::RB * W * sizeof(Real);
-        tma_load_3d(st + Cfg::TILE_C + offc, &m1, &bars[s], ti * W * 2, y, z);
+        if constexpr (!PD) tma_load_3d(st + Cfg::TILE_C + offc, &m1, &bars[s], ti * W * 2, y, z);
         if constexpr (OPS != 0) continue;
         tma_load_3d(st + 2 * Cfg::TILE_C + offr, &m2, &bars[s], ti * W, y, z);
         tma_load_3d(st + 2 * Cfg::TILE_C + Cfg::TILE_R + offr, &m3, &bars[s], ti * W, y, z);
@@ -206,6 +226,14 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
       // radial operators: gather from L2 before the transform so the loads
       // overlap it (z pass: kx = column, ky = outer index, kz = p)
       Real rla[RADIAL ? E : 1], rlb[RADIAL ? E : 1], rch[RADIAL && Cfg::CHI ? E : 1];
+      // PD: the state of this tile straight from HBM into registers, in flight
+      // during the forward transform
+      C pp[PD ? E : 1];
+      if constexpr (PD) {
+        const C *gph = reinterpret_cast<const C *>(a.psi_hat);
+#pragma unroll
+        for (int m = 0; m < E; ++m) pp[m] = gph[base + (long long)(j + T * m) * fs];
+      }
       if constexpr (RADIAL) {
 #pragma unroll
         for (int m = 0; m < E; ++m) {
@@ -214,7 +242,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
           if constexpr (Cfg::CHI) rch[m] = ch;
         }
       }
-      fft_line<C, N, -1, N>(v, tin, W, c, j, tw);
+      upd_fft<C, N, -1, TWR>(v, tin, W, c, j, tw, twr);
       const C *tpsi = reinterpret_cast<const C *>(st + Cfg::TILE_C);
       const Real *ta = reinterpret_cast<const Real *>(st + 2 * Cfg::TILE_C);
       const Real *tb = ta + N * W;
@@ -224,13 +252,17 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int e = (j + T * m) * W + c;
-        const C p = tpsi[e];
+        C p;
+        if constexpr (PD)
+          p = pp[m];
+        else
+          p = tpsi[e];
         Real la, lb, ch = Real(1);
         if constexpr (RADIAL) {
           la = rla[m];
           lb = rlb[m];
           if constexpr (Cfg::CHI) ch = rch[m];
-        } else if constexpr (OPS == 2) {
+        } else if constexpr (COMPUTED) {
           computed_ops<Real, MODEL>(a, ti * W + c, to, j + T * m, la, lb, ch);
         } else {
           la = ta[e];
@@ -244,16 +276,16 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
       }
       if constexpr (INV) {
         if constexpr (MODEL == MK_FILTERED) {
-          fft_line<C, N, +1, N>(w, tin, W, c, j, tw);
+          upd_fft<C, N, +1, TWR>(w, tin, W, c, j, tw, twr);
 #pragma unroll
           for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = w[m];
         } else {
-          fft_line<C, N, +1, N>(v, tin, W, c, j, tw);
+          upd_fft<C, N, +1, TWR>(v, tin, W, c, j, tw, twr);
 #pragma unroll
           for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
           if constexpr (MODEL == MK_TUNGSTEN) {
             C *gout2 = reinterpret_cast<C *>(a.out[1]);
-            fft_line<C, N, +1, N>(w, tin, W, c, j, tw);
+            upd_fft<C, N, +1, TWR>(w, tin, W, c, j, tw, twr);
 #pragma unroll
             for (int m = 0; m < E; ++m) gout2[base + (long long)(j + T * m) * fs] = w[m];
           }
@@ -299,7 +331,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
         for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
       }
     } else {
-      fft_line<C, N, -1, N>(v, sm, W, c, j, tw);
+      upd_fft<C, N, -1, TWR>(v, sm, W, c, j, tw, twr);
       C *ph = reinterpret_cast<C *>(a.psi_hat);
       C w[Cfg::CHI ? E : 1];
 #pragma unroll
@@ -312,7 +344,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
           Real la, lb;
           if constexpr (RADIAL) {
             radial_ops(a, a.rad_M, cg, j + T * m, la, lb, ch);  // Nyquist plane: kx = M, ky = column
-          } else if constexpr (OPS == 2) {
+          } else if constexpr (COMPUTED) {
             computed_ops<Real, MODEL>(a, a.rad_M, cg, j + T * m, la, lb, ch);
           } else {
             la = a.tab_a[idx];
@@ -327,20 +359,20 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
       }
       if constexpr (INV) {
         if constexpr (MODEL == MK_FILTERED) {
-          fft_line<C, N, +1, N>(w, sm, W, c, j, tw);
+          upd_fft<C, N, +1, TWR>(w, sm, W, c, j, tw, twr);
           if (ok) {
 #pragma unroll
             for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = w[m];
           }
         } else {
-          fft_line<C, N, +1, N>(v, sm, W, c, j, tw);
+          upd_fft<C, N, +1, TWR>(v, sm, W, c, j, tw, twr);
           if (ok) {
 #pragma unroll
             for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
           }
           if constexpr (MODEL == MK_TUNGSTEN) {
             C *gout2 = reinterpret_cast<C *>(a.out[1]);
-            fft_line<C, N, +1, N>(w, sm, W, c, j, tw);
+            upd_fft<C, N, +1, TWR>(w, sm, W, c, j, tw, twr);
             if (ok) {
 #pragma unroll
               for (int m = 0; m < E; ++m) gout2[base + (long long)(j + T * m) * fs] = w[m];

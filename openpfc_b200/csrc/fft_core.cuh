@@ -301,4 +301,97 @@ __device__ __forceinline__ void fft_line_e(C (&v)[E], C *sm, int ld, int c, int 
   fft_run<C, N, E, DIR, TWS>(typename PlanE<N, E>::R{}, v, sm, ld, c, j, tw);
 }
 
+// ---------------------------------------------------------------------------
+// Register-resident twiddles.  A thread's stage twiddles depend only on its
+// line position j, so a persistent kernel can load them once (TwReg::load) and
+// run every later transform of the same length from registers (fft_line_rt),
+// both directions (the inverse uses the conjugates).  Count per thread:
+// sum over stages with Ns > 1 of (E/R)(R-1).
+// ---------------------------------------------------------------------------
+template <int E, int... Rs> constexpr int tw_count(Radices<Rs...>) {
+  constexpr int rs[] = {1, Rs...};
+  int ns = 1, cnt = 0;
+  for (int i = 1; i <= (int)sizeof...(Rs); ++i) {
+    if (ns > 1) cnt += (E / rs[i]) * (rs[i] - 1);
+    ns *= rs[i];
+  }
+  return cnt;
+}
+
+template <typename C, int N, int E, int TWS, int Ns, int OFF, int CNT, int R, int... Rest>
+__device__ __forceinline__ void tw_load(C (&w)[CNT], int j, const C *tw) {
+  constexpr int T = N / E;
+  constexpr int B = E / R;
+  if constexpr (Ns > 1) {
+#pragma unroll
+    for (int t = 0; t < B; ++t) {
+      const int k = (j + t * T) % Ns;
+#pragma unroll
+      for (int r = 1; r < R; ++r) w[OFF + t * (R - 1) + r - 1] = tw[k * r * (TWS / (Ns * R))];
+    }
+  }
+  if constexpr (sizeof...(Rest) > 0)
+    tw_load<C, N, E, TWS, Ns * R, OFF + (Ns > 1 ? B * (R - 1) : 0), CNT, Rest...>(w, j, tw);
+}
+
+// stages() with the twiddles taken from the register cache w
+template <typename C, int N, int E, int DIR, int Ns, int OFF, int CNT, int R, int... Rest>
+__device__ __forceinline__ void stages_rt(C (&v)[E], C *sm, int ld, int c, int j, const C (&w)[CNT]) {
+  constexpr int T = N / E;
+  constexpr int B = E / R;
+  constexpr bool last = sizeof...(Rest) == 0;
+#pragma unroll
+  for (int t = 0; t < B; ++t) {
+    C x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = v[t + r * B];
+    const int b = j + t * T;
+    const int k = (Ns > 1) ? (b % Ns) : 0;
+    if constexpr (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) x[r] = twmul<DIR>(x[r], w[OFF + t * (R - 1) + r - 1]);
+    }
+    Dft<R, DIR, C>::run(x);
+    if constexpr (last) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[t + r * B] = x[r];
+    } else {
+      const int base = (b / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) sm[(base + r * Ns) * ld + c] = x[r];
+    }
+  }
+  if constexpr (!last) {
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = sm[(j + T * m) * ld + c];
+    __syncthreads();
+    stages_rt<C, N, E, DIR, Ns * R, OFF + (Ns > 1 ? B * (R - 1) : 0), CNT, Rest...>(v, sm, ld, c, j, w);
+  }
+}
+
+template <typename C, int N> struct TwReg {
+  static constexpr int E = Plan<N>::E;
+  static constexpr int CNT = tw_count<E>(typename Plan<N>::R{});
+  C w[CNT > 0 ? CNT : 1];
+  template <int... Rs> __device__ __forceinline__ void load_(Radices<Rs...>, int j, const C *tw) {
+    if constexpr (CNT > 0 && sizeof...(Rs) > 0) tw_load<C, N, E, N, 1, 0, CNT, Rs...>(w, j, tw);
+  }
+  __device__ __forceinline__ void load(int j, const C *tw) { load_(typename Plan<N>::R{}, j, tw); }
+};
+
+template <typename C, int N, int DIR, int... Rs>
+__device__ __forceinline__ void fft_rt_run(Radices<Rs...>, C (&v)[Plan<N>::E], C *sm, int ld, int c, int j,
+                                           const TwReg<C, N> &w) {
+  if constexpr (sizeof...(Rs) > 0)
+    stages_rt<C, N, Plan<N>::E, DIR, 1, 0, (TwReg<C, N>::CNT > 0 ? TwReg<C, N>::CNT : 1), Rs...>(v, sm, ld, c, j,
+                                                                                                 w.w);
+}
+
+// fft_line<C, N, DIR, N> with the twiddles from a TwReg cache
+template <typename C, int N, int DIR>
+__device__ __forceinline__ void fft_line_rt(C (&v)[Plan<N>::E], C *sm, int ld, int c, int j, const TwReg<C, N> &w) {
+  fft_rt_run<C, N, DIR>(typename Plan<N>::R{}, v, sm, ld, c, j, w);
+}
+
 }  // namespace opfc

@@ -40,14 +40,20 @@ template <typename Real> struct ColArgs {
 };
 
 // Operator selection of the fused z update.
-enum OpsKind { OPS_TABLES = 0, OPS_RADIAL = 1, OPS_COMPUTED = 2 };
+// OPS_COMPUTED_PD: computed operators, psi_hat prefetched into registers.
+enum OpsKind { OPS_TABLES = 0, OPS_RADIAL = 1, OPS_COMPUTED = 2, OPS_COMPUTED_PD = 3 };
 
 // Plain-PFC operators of mode (kx, ky, kz) (kx unfolded, ky / kz folded), in
 // the compute precision (10_complete_pfc_model.cpp:189-207, kspace.hpp:97-103):
 //   k^2 = sum (f_a i_a)^2, g = r + (1 - k^2)^2, L = -k^2 g,
 //   opL = exp(L dt),  opN = (opL - 1)/L (-k^2) = expm1(L dt)/g  (|L| > 1e-14),
 //   opN = dt (-k^2) otherwise;  FILTERED: chi = exp(-k^2 / (2 alpha^2)).
-// expm1 keeps the long-wavelength modes (|L dt| << 1) accurate in FP32.
+// One expm1 gives both: opL = 1 + expm1(L dt) (within half an ulp of 1 of
+// exp), and expm1 keeps the long-wavelength modes (|L dt| << 1) accurate in
+// FP32.  FP32 divides with the fast reciprocal (2 ulp); FP64 divides exactly.
+__device__ __forceinline__ float ops_div(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double ops_div(double a, double b) { return a / b; }
+
 template <typename Real, int MODEL>
 __device__ __forceinline__ void computed_ops(const ColArgs<Real> &a, int kx, int ky, int kz, Real &la,
                                              Real &lb, Real &ch) {
@@ -58,9 +64,9 @@ __device__ __forceinline__ void computed_ops(const ColArgs<Real> &a, int kx, int
   const Real u = Real(1) - k2;
   const Real g = a.op_r + u * u;
   const Real L = -k2 * g;
-  const Real x = L * a.op_dt;
-  la = exp(x);
-  lb = fabs(L) > Real(1e-14) ? expm1(x) / g : -a.op_dt * k2;
+  const Real em1 = expm1(L * a.op_dt);
+  la = Real(1) + em1;
+  lb = fabs(L) > Real(1e-14) ? ops_div(em1, g) : -a.op_dt * k2;
   ch = MODEL == MK_FILTERED ? exp(-k2 * a.op_chi) : Real(1);
 }
 
@@ -599,14 +605,16 @@ static int launch_col_direct(const ColLaunch &L, cudaStream_t s) {
 template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS, bool NARROW>
 static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
   using C = typename Cx<Real>::T;
-  constexpr int W = tma_col_width(N, (int)sizeof(C), MODE, NARROW);
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS>;
+  constexpr int W = tma_col_width(N, (int)sizeof(C), MODE, NARROW, OPS == OPS_COMPUTED_PD);
   constexpr int NT = W * (N / Plan<N>::E);
-  // narrow tiles: two CTAs per SM when their shared memory fits and each has at
-  // most 512 threads (64 registers per thread)
-  constexpr int MINB = (NARROW && 2 * (Cfg::SMEM + 1024) <= 233472 && NT <= 512) ? 2 : 1;
+  // NARROW: two CTAs per SM when their shared memory fits and each has at most
+  // 512 threads (64 registers per thread); plain transforms take half-width
+  // tiles, the update keeps its width with one stage per CTA
+  using Cfg2 = TmaCfg<Real, N, W, MODE, MODEL, OPS, MODE == COL_UPDATE ? 1 : 3>;
+  constexpr int MINB = (NARROW && Cfg2::STAGES >= 1 && 2 * (Cfg2::SMEM + 1024) <= 233472 && NT <= 512) ? 2 : 1;
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, (MINB > 1 && MODE == COL_UPDATE) ? 1 : 3>;
   if constexpr (Cfg::STAGES < 1 || (NARROW && MINB < 2) ||
-                (OPS == OPS_COMPUTED && MODEL == MK_TUNGSTEN)) {
+                (OPS >= OPS_COMPUTED && MODEL == MK_TUNGSTEN)) {
     return -1;
   } else {
     if (L.seg[0].ncols % W != 0 || L.seg[0].col_stride != 1) return -1;
@@ -639,7 +647,9 @@ static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
     int rc;
     if constexpr (MODE == COL_UPDATE)
       rc = L.rad_ops    ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_RADIAL, false>(L, s)
-           : L.computed ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false>(L, s)
+           : L.computed ? (L.narrow       ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, true>(L, s)
+                           : L.psi_direct ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED_PD, false>(L, s)
+                                          : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false>(L, s))
                         : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false>(L, s);
     else
       rc = L.narrow ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, true>(L, s)
@@ -694,12 +704,12 @@ template <typename Real> static XArgs<Real> x_args(const XLaunch &L) {
   return a;
 }
 
-template <typename Real, int R, int MODEL>
+template <typename Real, int R, int MODEL, int H = 1>
 static int launch_x_sq(const XLaunch &L, cudaStream_t s) {
-  using Cfg = XSqCfg<Real, R, MODEL>;
+  using Cfg = XSqCfg<Real, R, MODEL, H>;
   if (L.rows % Cfg::W != 0 || Cfg::SMEM > (size_t)kMaxDynSmem) return -1;
   constexpr int NT = Cfg::W * R;
-  auto k = x_sq_kernel<Real, R, MODEL>;
+  auto k = x_sq_kernel<Real, R, MODEL, H>;
   static int occ = 0;
   if (!occ) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
@@ -797,11 +807,21 @@ static int launch_x_m(const XLaunch &L, cudaStream_t s) {
     int rc = -1;
     if constexpr (M == 64 || M == 256) {
       constexpr int R = M == 64 ? 8 : 16;
-      switch (L.model) {
-        case MK_PLAIN: rc = launch_x_sq<Real, R, MK_PLAIN>(L, s); break;
-        case MK_TUNGSTEN: rc = launch_x_sq<Real, R, MK_TUNGSTEN>(L, s); break;
-        case MK_FILTERED: rc = launch_x_sq<Real, R, MK_FILTERED>(L, s); break;
-      }
+      if (!L.no_sq) switch (L.model) {
+          case MK_PLAIN: rc = launch_x_sq<Real, R, MK_PLAIN>(L, s); break;
+          case MK_TUNGSTEN: rc = launch_x_sq<Real, R, MK_TUNGSTEN>(L, s); break;
+          case MK_FILTERED: rc = launch_x_sq<Real, R, MK_FILTERED>(L, s); break;
+        }
+      if (rc >= 0) return rc;
+    }
+    // M = 2 R^2 (FP32, one field per row): radix-2 around two R^2 transforms
+    if constexpr ((M == 128 || M == 512) && sizeof(Real) == 4) {
+      constexpr int R = M == 128 ? 8 : 16;
+      if (!L.no_sq) switch (L.model) {
+          case MK_PLAIN: rc = launch_x_sq<Real, R, MK_PLAIN, 2>(L, s); break;
+          case MK_FILTERED: rc = launch_x_sq<Real, R, MK_FILTERED, 2>(L, s); break;
+          default: break;
+        }
       if (rc >= 0) return rc;
     }
     switch (L.model) {

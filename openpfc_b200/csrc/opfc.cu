@@ -36,7 +36,7 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 3, kVarX = 2, kVarZ = 5;  // kernel variants per pass (opfc_autotune)
+constexpr int kVarY = 3, kVarX = 3, kVarZ = 7;  // kernel variants per pass (opfc_autotune)
 
 bool supported_len(int n) {
   static const int ok[] = {1, 2, 4, 8, 16, 24, 32, 40, 48, 64, 80, 96, 128, 256, 512, 1024};
@@ -127,10 +127,13 @@ struct opfc_handle {
   bool use_tma = true;  // TMA-fed column passes (OPFC_NO_TMA=1 disables)
   // kernel variants per pass, chosen by the autotuner (see opfc_autotune):
   // var_y: 0 pipelined, 1 direct, 2 pipelined narrow tiles (two CTAs per SM);
-  // var_x: 0 pipelined, 1 direct;
+  // var_x: 0 pipelined (warp-square kernel where it applies), 1 direct,
+  //        2 pipelined without the warp-square kernel;
   // var_z: 0 pipelined with streamed tables, 1 pipelined with radial tables,
   //        2 direct with streamed tables, 3 pipelined with computed operators,
-  //        4 direct with computed operators (3, 4: PLAIN and FILTERED)
+  //        4 direct with computed operators, 5 pipelined with computed operators
+  //        and two CTAs per SM, 6 pipelined A with psi_hat prefetched into
+  //        registers and computed operators (3-6: PLAIN and FILTERED)
   int var_y = 0, var_x = 0, var_z = 0;
   int num_sms = 148;
   struct Tmap {
@@ -348,7 +351,8 @@ XLaunch x_base(opfc_handle *h) {
   L.scale = 1.0 / ((double)h->n0 * h->n1 * h->n2);
   L.mean = 0.0;
   L.flag = h->flag;
-  L.use_tma = h->use_tma && h->var_x == 0;
+  L.use_tma = h->use_tma && h->var_x != 1;
+  L.no_sq = h->var_x == 2;
   L.num_sms = h->num_sms;
   return L;
 }
@@ -461,7 +465,9 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.tab_chi = h->tab_chi;
     Z.axis = 2;
     // computed operators (variants 3, 4): PLAIN and FILTERED models
-    Z.computed = (h->var_z == 3 || h->var_z == 4) && model != OPFC_MODEL_TUNGSTEN;
+    Z.computed = h->var_z >= 3 && model != OPFC_MODEL_TUNGSTEN;
+    Z.narrow = h->var_z == 5;
+    Z.psi_direct = h->var_z == 6;
     Z.rad_M = h->M;
     Z.rad_n1 = h->n1;
     Z.rad_n2 = h->n2;
@@ -470,12 +476,12 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.op_r = h->desc.r;
     Z.op_dt = h->dt;
     Z.op_chi = model == OPFC_MODEL_FILTERED ? 1.0 / (2.0 * h->desc.filter_alpha * h->desc.filter_alpha) : 0.0;
-    const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE);
+    const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE, false, Z.psi_direct != 0);
     if (h->use_tma && h->var_z != 2 && h->var_z != 4 && Z.N > 1 && h->M % W == 0) {
       Z.tmap[0] = tmap_for(h, h->work_a, 2, W, false);
       Z.tmap[1] = tmap_for(h, h->psi_hat, 2, W, false);
       if (Z.computed) {
-        if (!Z.tmap[1]) Z.tmap[0] = nullptr;
+        if (!Z.tmap[1]) Z.tmap[0] = nullptr;  // (psi_direct: m1 is passed but not read)
       } else if (h->rad_ops && h->var_z == 1) {
         // isotropic grid: operators from the L2-resident radial tables
         Z.rad_ops = h->rad_ops;
@@ -966,12 +972,14 @@ int opfc_initialize(opfc_handle *h, double dt) {
   }
   h->dt = dt;
   // kernel variants: the autotuner's cached choice, else the defaults;
-  // OPFC_Z_VARIANT / OPFC_Y_VARIANT force the z-update / y-pass variant
+  // OPFC_Y_VARIANT / OPFC_X_VARIANT / OPFC_Z_VARIANT force a pass's variant
   h->var_y = AutoTuner::instance().get_config(tune_key(h, "y"), 0);
   h->var_x = AutoTuner::instance().get_config(tune_key(h, "x"), 0);
   h->var_z = AutoTuner::instance().get_config(tune_key(h, "z"), 0);
   if (const char *zv = std::getenv("OPFC_Z_VARIANT")) h->var_z = std::atoi(zv);
   if (const char *yv = std::getenv("OPFC_Y_VARIANT")) h->var_y = std::atoi(yv);
+  if (const char *xv = std::getenv("OPFC_X_VARIANT")) h->var_x = std::atoi(xv);
+  if (h->var_x < 0 || h->var_x >= kVarX) h->var_x = 0;
   if (h->var_z == 1 && !h->rad_ops) h->var_z = 0;
   if (h->var_z >= 3 && model == OPFC_MODEL_TUNGSTEN) h->var_z = h->var_z == 4 ? 2 : 0;
   if (h->var_z < 0 || h->var_z >= kVarZ) h->var_z = 0;

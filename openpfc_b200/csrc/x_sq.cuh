@@ -1,5 +1,5 @@
-// x_sq.cuh -- fused x pass for half lengths M = R*R (R = 8, 16): one x-row is
-// owned by R lanes of one warp.
+// x_sq.cuh -- fused x pass for half lengths M = H*R*R (R = 8, 16; H = 1, 2): one
+// x-row is owned by R lanes of one warp, each holding E = H*R values.
 //
 // The complex FFT of length M is a two-stage Stockham (radix R, then radix R
 // with twiddles W_M^{j r}); its single exchange is a padded R x (R+1) transpose
@@ -9,15 +9,23 @@
 // post-processing pairs Z[k] with Z[M-k] through warp shuffles (lane j holds
 // k = j + R m, its partner is lane R-j), and stores the modes straight to HBM.
 // Tiles of W rows arrive by cp.async.bulk exactly as in x_tma.cuh.
+//
+// H = 2 (M = 2 R^2): the inverse transform is one radix-2 decimation-in-
+// frequency step (pairs p, p + M/2 sit in the same lane) followed by two
+// length-R^2 transforms, which leaves the even and odd output positions in the
+// two register halves; the nonlinearity is pointwise, and the forward transform
+// is the matching decimation-in-time form (two length-R^2 transforms of the
+// even / odd halves, then the radix-2 combine), which returns natural order.
 #pragma once
 #include "x_tma.cuh"
 
 namespace opfc {
 
-template <typename Real, int R, int MODEL> struct XSqCfg {
+template <typename Real, int R, int MODEL, int H = 1> struct XSqCfg {
   using C = typename CxP<Real>::T;
-  static constexpr int M = R * R;
-  static constexpr int W = Width<Real>::W;  // rows (lines) per tile
+  static constexpr int M = H * R * R;
+  static constexpr int E = H * R;                // values per lane
+  static constexpr int W = Width<Real>::W / H;  // rows (lines) per tile
   static constexpr int P = M + 2;           // padded row pitch of the landed tile
   static constexpr int EXL = R * (R + 1);   // exchange space per line
   static constexpr size_t TILE = (size_t(W) * P + W) * sizeof(C);
@@ -56,11 +64,68 @@ __device__ __forceinline__ void fft_sq(C (&v)[R], C *ex, int j, const C *tws) {
   Dft<R, DIR, C>::run(v);  // stage 2 (Ns = R): outputs x[j + R r]
 }
 
-template <typename Real, int R, int MODEL>
-__global__ void __launch_bounds__(Width<Real>::W *R) x_sq_kernel(const XArgs<Real> a) {
-  using Cfg = XSqCfg<Real, R, MODEL>;
+// Length H*R*R inverse-style transform: natural order in (v[m] = x[j + R m],
+// m < H R); H = 2 leaves the even outputs in v[0, R) and the odd ones in v[R, 2R)
+// (v[m] = X[2 (j + R m)], v[R + m] = X[2 (j + R m) + 1]).  tw = W_{2M}^k, k < M.
+template <typename C, int R, int H, int DIR>
+__device__ __forceinline__ void fft_sq_dif(C (&v)[H * R], C *ex, int j, const C *tws, const C *tw) {
+  if constexpr (H == 1) {
+    fft_sq<C, R, DIR>(v, ex, j, tws);
+  } else {
+#pragma unroll
+    for (int m = 0; m < R; ++m) {  // p = j + R m and p + M/2 share the lane
+      const C a = v[m], b = v[m + R];
+      v[m] = cadd(a, b);
+      v[m + R] = twmul<DIR>(csub(a, b), tw[2 * (j + R * m)]);  // W_M^p
+    }
+    C h[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) h[m] = v[m];
+    fft_sq<C, R, DIR>(h, ex, j, tws);
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      v[m] = h[m];
+      h[m] = v[m + R];
+    }
+    fft_sq<C, R, DIR>(h, ex, j, tws);
+#pragma unroll
+    for (int m = 0; m < R; ++m) v[m + R] = h[m];
+  }
+}
+
+// The matching forward-style transform: even / odd halves in (as fft_sq_dif
+// leaves them), natural order out.
+template <typename C, int R, int H, int DIR>
+__device__ __forceinline__ void fft_sq_dit(C (&v)[H * R], C *ex, int j, const C *tws, const C *tw) {
+  if constexpr (H == 1) {
+    fft_sq<C, R, DIR>(v, ex, j, tws);
+  } else {
+    C h[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) h[m] = v[m];
+    fft_sq<C, R, DIR>(h, ex, j, tws);
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+      v[m] = h[m];
+      h[m] = v[m + R];
+    }
+    fft_sq<C, R, DIR>(h, ex, j, tws);
+#pragma unroll
+    for (int m = 0; m < R; ++m) {  // X[k] = A[k] + W_M^k B[k], X[k + M/2] = A[k] - W_M^k B[k]
+      const C t = twmul<DIR>(h[m], tw[2 * (j + R * m)]);
+      const C a0 = v[m];
+      v[m] = cadd(a0, t);
+      v[m + R] = csub(a0, t);
+    }
+  }
+}
+
+template <typename Real, int R, int MODEL, int H>
+__global__ void __launch_bounds__(XSqCfg<Real, R, MODEL, H>::W *R) x_sq_kernel(const XArgs<Real> a) {
+  using Cfg = XSqCfg<Real, R, MODEL, H>;
   using C = typename CxP<Real>::T;
   constexpr int M = Cfg::M;
+  constexpr int E = Cfg::E;
   constexpr int W = Cfg::W;
   constexpr int NT = W * R;
   constexpr int N0 = 2 * M;
@@ -80,7 +145,7 @@ __global__ void __launch_bounds__(Width<Real>::W *R) x_sq_kernel(const XArgs<Rea
   for (int i = tid; i < M; i += NT) tw[i] = gtw[i];
   for (int i = tid; i < (R - 1) * R; i += NT) {
     const int r = i / R + 1, k = i % R;
-    tws[i] = gtw[(2 * k * r) % N0];  // W_M^{k r} = exp(-2 pi i k r / M)
+    tws[i] = gtw[((N0 / (R * R)) * k * r) % N0];  // W_{R^2}^{k r} = exp(-2 pi i k r / R^2)
   }
   if (tid == 0) {
     for (int s = 0; s < STAGES; ++s) mbar_init(&bars[s], 1);
@@ -122,19 +187,21 @@ __global__ void __launch_bounds__(Width<Real>::W *R) x_sq_kernel(const XArgs<Rea
     }
     unsigned char *st = stage0 + s * Cfg::STAGE;
     C *buf0 = reinterpret_cast<C *>(st);
-    C v[R];
-    x_pre_rows<C, M, Cfg::P, R>(buf0, buf0 + W * Cfg::P, tw, c, j, v);
+    C *ex0 = buf0 + c * Cfg::EXL;
+    C v[E];
+    x_pre_rows<C, M, Cfg::P, E>(buf0, buf0 + W * Cfg::P, tw, c, j, v);
     if constexpr (MODEL == MK_TUNGSTEN) {
+      static_assert(H == 1, "two-field rows use H = 1");
       C *buf1 = reinterpret_cast<C *>(st + Cfg::BUF);
-      C u[R];
-      x_pre_rows<C, M, Cfg::P, R>(buf1, buf1 + W * Cfg::P, tw, c, j, u);
+      C u[E];
+      x_pre_rows<C, M, Cfg::P, E>(buf1, buf1 + W * Cfg::P, tw, c, j, u);
       __syncthreads();  // landed rows consumed: the buffers become exchange space
-      fft_sq<C, R, +1>(v, buf0 + c * Cfg::EXL, j, tws);
+      fft_sq<C, R, +1>(v, ex0, j, tws);
       fft_sq<C, R, +1>(u, buf1 + c * Cfg::EXL, j, tws);
       // N = p3b u^2 + p4b u^3 + q3b v^2 + q4b v^3 - stabP u with u = psi, v = psi_MF
       // (apps/tungsten/include/tungsten/cpu/tungsten_model.hpp:334-350)
 #pragma unroll
-      for (int m = 0; m < R; ++m) {
+      for (int m = 0; m < E; ++m) {
         const Real ux = v[m].x * sc + mn, uy = v[m].y * sc + mn;
         const Real vx = u[m].x * sc + mn, vy = u[m].y * sc + mn;
         const Real nx = ux * ux * (a.c0 + a.c1 * ux) + vx * vx * (a.c2 + a.c3 * vx) - a.c4 * ux;
@@ -144,9 +211,9 @@ __global__ void __launch_bounds__(Width<Real>::W *R) x_sq_kernel(const XArgs<Rea
       }
     } else {
       __syncthreads();
-      fft_sq<C, R, +1>(v, buf0 + c * Cfg::EXL, j, tws);
+      fft_sq_dif<C, R, H, +1>(v, ex0, j, tws, tw);
 #pragma unroll
-      for (int m = 0; m < R; ++m) {
+      for (int m = 0; m < E; ++m) {
         const Real x = v[m].x * sc + mn, y = v[m].y * sc + mn;
         Real nx, ny;
         if constexpr (MODEL == MK_FILTERED) {
@@ -160,14 +227,15 @@ __global__ void __launch_bounds__(Width<Real>::W *R) x_sq_kernel(const XArgs<Rea
         v[m] = mk<C>(nx, ny);
       }
     }
-    fft_sq<C, R, -1>(v, buf0 + c * Cfg::EXL, j, tws);
-    // R2C post-processing: X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W_N0^k (Z[k] - conj Z[M-k])
+    fft_sq_dit<C, R, H, -1>(v, ex0, j, tws, tw);
+    // R2C post-processing: X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W_N0^k (Z[k] - conj Z[M-k]);
+    // lane j holds k = j + R m, Z[M - k] is element E-1-m of lane R-j (lane 0: element E-m)
     const long long row = (long long)t * W + c;
 #pragma unroll
-    for (int m = 0; m < R; ++m) {
+    for (int m = 0; m < E; ++m) {
       const int k = j + R * m;
-      C Y = shfl_c(v[R - 1 - m], partner);
-      if (j == 0) Y = v[(R - m) % R];
+      C Y = shfl_c(v[E - 1 - m], partner);
+      if (j == 0) Y = v[(E - m) % E];
       const C Z = v[m];
       const C sm = mk<C>(Z.x + Y.x, Z.y - Y.y);
       const C d = mk<C>(Z.x - Y.x, Z.y + Y.y);

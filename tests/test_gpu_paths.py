@@ -14,19 +14,23 @@ pytestmark = pytest.mark.gpu
 PI4 = [math.pi / 4] * 3
 
 
-@pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed"])
+@pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "psi_direct"])
 def path(request, monkeypatch):
     """tma: pipelined kernels streaming the per-mode tables (default);
     tma_radial: the z update reading radial operator tables (OPFC_Z_VARIANT=1,
     isotropic grids; others fall back to tables);
     direct: direct-load kernels (OPFC_NO_TMA=1);
     computed: pipelined z update computing its operators from k^2
-    (OPFC_Z_VARIANT=3) and half-width y tiles (OPFC_Y_VARIANT=2);
-    direct_computed: direct z update computing its operators (OPFC_Z_VARIANT=4).
+    (OPFC_Z_VARIANT=3), half-width y tiles (OPFC_Y_VARIANT=2) and the x pass
+    without the warp-square kernel (OPFC_X_VARIANT=2);
+    direct_computed: direct z update computing its operators (OPFC_Z_VARIANT=4);
+    psi_direct: pipelined z update with psi_hat prefetched into registers
+    (OPFC_Z_VARIANT=6).
     The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
     monkeypatch.delenv("OPFC_Y_VARIANT", raising=False)
+    monkeypatch.delenv("OPFC_X_VARIANT", raising=False)
     monkeypatch.setenv("OPENPFC_GPU_AUTOTUNE_MODE", "fallback_only")
     if request.param == "direct":
         monkeypatch.setenv("OPFC_NO_TMA", "1")
@@ -35,8 +39,11 @@ def path(request, monkeypatch):
     elif request.param == "computed":
         monkeypatch.setenv("OPFC_Z_VARIANT", "3")
         monkeypatch.setenv("OPFC_Y_VARIANT", "2")
+        monkeypatch.setenv("OPFC_X_VARIANT", "2")
     elif request.param == "direct_computed":
         monkeypatch.setenv("OPFC_Z_VARIANT", "4")
+    elif request.param == "psi_direct":
+        monkeypatch.setenv("OPFC_Z_VARIANT", "6")
     return request.param
 
 
@@ -45,7 +52,7 @@ def rel_l2(a, b):
 
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
-@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 256), (256, 16, 512), (512, 32, 16)])
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 256), (256, 16, 512), (512, 32, 16), (1024, 16, 16)])
 def test_plain(oracle, path, prec, tol, n):
     psi0 = oracle.ic_noise(n, -0.285, 0.01, 3)
     ref = oracle.run_plain(psi0, PI4, -0.25, 0.5, 10)
@@ -58,7 +65,7 @@ def test_plain(oracle, path, prec, tol, n):
 
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
-@pytest.mark.parametrize("n", [(64, 64, 32), (512, 16, 16), (128, 32, 32)])
+@pytest.mark.parametrize("n", [(64, 64, 32), (512, 16, 16), (128, 32, 32), (1024, 16, 8)])
 def test_filtered(oracle, path, prec, tol, n):
     psi0 = oracle.ic_seeds(n, PI4, -0.10, 0.001, 2, 8.0, 0.2, 4)
     ref = oracle.run_filtered(psi0, PI4, -0.3, 0.5, -0.1, -0.5, 0.3, 0.5, 10)
