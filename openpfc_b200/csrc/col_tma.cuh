@@ -76,7 +76,8 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
 constexpr size_t align128(size_t b) { return (b + 127) & ~size_t(127); }
 constexpr int kMaxDynSmem = 232448;  // 227 KB opt-in per CTA on sm_100
 
-template <typename Real, int N, int W, int MODE, int MODEL, int OPS = 0, int SCAP = 3> struct TmaCfg {
+template <typename Real, int N, int W, int MODE, int MODEL, int OPS = 0, int SCAP = 3, bool PP = false>
+struct TmaCfg {
   using C = typename Cx<Real>::T;
   static constexpr bool UPD = MODE == COL_UPDATE;
   static constexpr bool CHI = UPD && MODEL != MK_PLAIN;
@@ -88,9 +89,11 @@ template <typename Real, int N, int W, int MODE, int MODEL, int OPS = 0, int SCA
   static constexpr size_t STAGE =
       TILE_C + (UPD ? (OPS == 3 ? 0 : TILE_C) + (OPS != 0 ? 0 : 2 * TILE_R + (CHI ? TILE_R : 0)) : 0);
   static constexpr size_t TW = align128(size_t(N) * sizeof(C));
-  static constexpr int S0 = int((kMaxDynSmem - TW - 128) / STAGE);
+  // PP: a second FFT exchange buffer (ping-pong with the landed tile)
+  static constexpr size_t XB = PP ? align128(TILE_C) : 0;
+  static constexpr int S0 = int((kMaxDynSmem - TW - XB - 128) / STAGE);
   static constexpr int STAGES = S0 > SCAP ? SCAP : S0;
-  static constexpr size_t SMEM = TW + size_t(STAGES > 0 ? STAGES : 1) * STAGE + 64;
+  static constexpr size_t SMEM = TW + XB + size_t(STAGES > 0 ? STAGES : 1) * STAGE + 64;
   static constexpr int RB = N < 256 ? N : 256;  // rows per TMA box (box dims <= 256)
   static constexpr int NB = N / RB;
 };
@@ -110,11 +113,14 @@ __device__ __forceinline__ void radial_ops(const ColArgs<Real> &a, int kx, int k
 }
 
 // Update-mode transform: stage twiddles from the register cache (TWR) or the
-// shared table.
-template <typename C, int N, int D, bool TWR>
+// shared table; PP exchanges through (buf, xb) in turn.
+// K = index of this transform within the tile (continues the exchange parity).
+template <typename C, int N, int D, bool TWR, bool PP = false, int K = 0>
 __device__ __forceinline__ void upd_fft(C (&x)[Plan<N>::E], C *buf, int ld, int c, int j, const C *tw,
-                                        const TwReg<C, N> &twr) {
-  if constexpr (TWR)
+                                        const TwReg<C, N> &twr, C *xb = nullptr) {
+  if constexpr (PP)
+    fft_line_pp<C, N, D, TWR, K * fft_exchanges<N>()>(x, buf, xb, ld, c, j, tw, twr);
+  else if constexpr (TWR)
     fft_line_rt<C, N, D>(x, buf, ld, c, j, twr);
   else
     fft_line<C, N, D, N>(x, buf, ld, c, j, tw);
@@ -123,14 +129,14 @@ __device__ __forceinline__ void upd_fft(C (&x)[Plan<N>::E], C *buf, int ld, int 
 // Tensor maps: PLAIN uses m0 (array set 0) and m1 (array set 1); UPDATE uses
 // m0 = N_hat partial (A), m1 = psi_hat, m2 = tab_a, m3 = tab_b, m4 = tab_chi
 // (m2..m4 unused unless OPS == 0, per-mode tables).  MINB CTAs share an SM.
-template <typename Real, int N, int W, int MODE, int DIR, int MODEL, bool INV, int OPS, int MINB>
+template <typename Real, int N, int W, int MODE, int DIR, int MODEL, bool INV, int OPS, int MINB, bool PP>
 __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
     col_tma_kernel(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
                    const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3,
                    const __grid_constant__ CUtensorMap m4, const ColArgs<Real> a, const int axis,
                    unsigned *flag) {
   // two CTAs per SM for the update: one stage each
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, (MINB > 1 && MODE == COL_UPDATE) ? 1 : 3>;
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, (MINB > 1 && MODE == COL_UPDATE) ? 1 : 3, PP>;
   using C = typename Cx<Real>::T;
   constexpr bool RADIAL = OPS == 1;
   constexpr bool COMPUTED = OPS == 2 || OPS == 3;
@@ -142,7 +148,8 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
   constexpr bool UPD = Cfg::UPD;
   extern __shared__ __align__(128) unsigned char smraw[];
   C *tw = reinterpret_cast<C *>(smraw);
-  unsigned char *stage0 = smraw + Cfg::TW;
+  C *xb = reinterpret_cast<C *>(smraw + Cfg::TW);  // PP exchange buffer (XB bytes)
+  unsigned char *stage0 = smraw + Cfg::TW + Cfg::XB;
   uint64_t *bars = reinterpret_cast<uint64_t *>(stage0 + STAGES * Cfg::STAGE);
 
   const int tid = threadIdx.x;
@@ -217,9 +224,13 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
     C v[E];
 #pragma unroll
     for (int m = 0; m < E; ++m) v[m] = tin[(j + T * m) * W + c];
-    __syncthreads();
+    // PP: the first exchange writes xb, so the tile needs no barrier here
+    if constexpr (!PP) __syncthreads();
     if constexpr (MODE == COL_PLAIN) {
-      fft_line<C, N, DIR, N>(v, tin, W, c, j, tw);
+      if constexpr (PP)
+        fft_line_pp<C, N, DIR, false>(v, tin, xb, W, c, j, tw, twr);
+      else
+        fft_line<C, N, DIR, N>(v, tin, W, c, j, tw);
 #pragma unroll
       for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
     } else {
@@ -242,7 +253,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
           if constexpr (Cfg::CHI) rch[m] = ch;
         }
       }
-      upd_fft<C, N, -1, TWR>(v, tin, W, c, j, tw, twr);
+      upd_fft<C, N, -1, TWR, PP, 0>(v, tin, W, c, j, tw, twr, xb);
       const C *tpsi = reinterpret_cast<const C *>(st + Cfg::TILE_C);
       const Real *ta = reinterpret_cast<const Real *>(st + 2 * Cfg::TILE_C);
       const Real *tb = ta + N * W;
@@ -276,16 +287,16 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
       }
       if constexpr (INV) {
         if constexpr (MODEL == MK_FILTERED) {
-          upd_fft<C, N, +1, TWR>(w, tin, W, c, j, tw, twr);
+          upd_fft<C, N, +1, TWR, PP, 1>(w, tin, W, c, j, tw, twr, xb);
 #pragma unroll
           for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = w[m];
         } else {
-          upd_fft<C, N, +1, TWR>(v, tin, W, c, j, tw, twr);
+          upd_fft<C, N, +1, TWR, PP, 1>(v, tin, W, c, j, tw, twr, xb);
 #pragma unroll
           for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
           if constexpr (MODEL == MK_TUNGSTEN) {
             C *gout2 = reinterpret_cast<C *>(a.out[1]);
-            upd_fft<C, N, +1, TWR>(w, tin, W, c, j, tw, twr);
+            upd_fft<C, N, +1, TWR, PP, 2>(w, tin, W, c, j, tw, twr, xb);
 #pragma unroll
             for (int m = 0; m < E; ++m) gout2[base + (long long)(j + T * m) * fs] = w[m];
           }

@@ -370,6 +370,67 @@ __device__ __forceinline__ void stages_rt(C (&v)[E], C *sm, int ld, int c, int j
   }
 }
 
+// ---------------------------------------------------------------------------
+// Ping-pong exchange: exchange e writes buffer (e even ? b1 : b0) and reads it
+// back, so one CTA barrier per exchange suffices (a buffer is rewritten only
+// two exchanges later, after a barrier every thread has passed since its last
+// read of it).  b0 may be the landed input tile: exchange 0 never writes it.
+// Twiddles from the shared table (TWR = false) or a TwReg cache (TWR = true).
+// ---------------------------------------------------------------------------
+template <typename C, int N, int E, int DIR, int TWS, bool TWR, int EX, int Ns, int OFF, int CNT, int R,
+          int... Rest>
+__device__ __forceinline__ void stages_pp(C (&v)[E], C *b0, C *b1, int ld, int c, int j, const C *tw,
+                                          const C (&w)[CNT]) {
+  constexpr int T = N / E;
+  constexpr int B = E / R;
+  constexpr bool last = sizeof...(Rest) == 0;
+  C *sm = (EX % 2 == 0) ? b1 : b0;
+#pragma unroll
+  for (int t = 0; t < B; ++t) {
+    C x[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) x[r] = v[t + r * B];
+    const int b = j + t * T;
+    const int k = (Ns > 1) ? (b % Ns) : 0;
+    if constexpr (Ns > 1) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        if constexpr (TWR)
+          x[r] = twmul<DIR>(x[r], w[OFF + t * (R - 1) + r - 1]);
+        else
+          x[r] = twmul<DIR>(x[r], tw[k * r * (TWS / (Ns * R))]);
+      }
+    }
+    Dft<R, DIR, C>::run(x);
+    if constexpr (last) {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[t + r * B] = x[r];
+    } else {
+      const int base = (b / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) sm[(base + r * Ns) * ld + c] = x[r];
+    }
+  }
+  if constexpr (!last) {
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = sm[(j + T * m) * ld + c];
+    stages_pp<C, N, E, DIR, TWS, TWR, EX + 1, Ns * R, OFF + (Ns > 1 ? B * (R - 1) : 0), CNT, Rest...>(
+        v, b0, b1, ld, c, j, tw, w);
+  }
+}
+
+template <typename C, int N, int DIR, bool TWR, int EX0, int CNT, int... Rs>
+__device__ __forceinline__ void fft_pp_run(Radices<Rs...>, C (&v)[Plan<N>::E], C *b0, C *b1, int ld, int c, int j,
+                                           const C *tw, const C (&w)[CNT]) {
+  if constexpr (sizeof...(Rs) > 0)
+    stages_pp<C, N, Plan<N>::E, DIR, N, TWR, EX0, 1, 0, CNT, Rs...>(v, b0, b1, ld, c, j, tw, w);
+}
+
+// shared-memory exchanges of one length-N transform
+template <int... Rs> constexpr int n_exchanges(Radices<Rs...>) { return sizeof...(Rs) > 0 ? int(sizeof...(Rs)) - 1 : 0; }
+template <int N> constexpr int fft_exchanges() { return n_exchanges(typename Plan<N>::R{}); }
+
 template <typename C, int N> struct TwReg {
   static constexpr int E = Plan<N>::E;
   static constexpr int CNT = tw_count<E>(typename Plan<N>::R{});
@@ -392,6 +453,17 @@ __device__ __forceinline__ void fft_rt_run(Radices<Rs...>, C (&v)[Plan<N>::E], C
 template <typename C, int N, int DIR>
 __device__ __forceinline__ void fft_line_rt(C (&v)[Plan<N>::E], C *sm, int ld, int c, int j, const TwReg<C, N> &w) {
   fft_rt_run<C, N, DIR>(typename Plan<N>::R{}, v, sm, ld, c, j, w);
+}
+
+// fft_line<C, N, DIR, N> with ping-pong exchange buffers (b0, b1); TWR selects
+// the twiddles of the TwReg cache w over the shared table tw.  Transforms run
+// back to back without a barrier between them continue the exchange count:
+// EX0 = exchanges made since the last CTA-wide barrier that ended a tile.
+template <typename C, int N, int DIR, bool TWR, int EX0 = 0>
+__device__ __forceinline__ void fft_line_pp(C (&v)[Plan<N>::E], C *b0, C *b1, int ld, int c, int j, const C *tw,
+                                            const TwReg<C, N> &w) {
+  constexpr int CNT = TwReg<C, N>::CNT > 0 ? TwReg<C, N>::CNT : 1;
+  fft_pp_run<C, N, DIR, TWR, EX0, CNT>(typename Plan<N>::R{}, v, b0, b1, ld, c, j, tw, w.w);
 }
 
 }  // namespace opfc

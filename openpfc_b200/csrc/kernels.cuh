@@ -602,7 +602,7 @@ static int launch_col_direct(const ColLaunch &L, cudaStream_t s) {
   return (int)cudaGetLastError();
 }
 
-template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS, bool NARROW>
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS, bool NARROW, bool PP = false>
 static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
   using C = typename Cx<Real>::T;
   constexpr int W = tma_col_width(N, (int)sizeof(C), MODE, NARROW, OPS == OPS_COMPUTED_PD);
@@ -610,15 +610,15 @@ static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
   // NARROW: two CTAs per SM when their shared memory fits and each has at most
   // 512 threads (64 registers per thread); plain transforms take half-width
   // tiles, the update keeps its width with one stage per CTA
-  using Cfg2 = TmaCfg<Real, N, W, MODE, MODEL, OPS, MODE == COL_UPDATE ? 1 : 3>;
+  using Cfg2 = TmaCfg<Real, N, W, MODE, MODEL, OPS, MODE == COL_UPDATE ? 1 : 3, PP>;
   constexpr int MINB = (NARROW && Cfg2::STAGES >= 1 && 2 * (Cfg2::SMEM + 1024) <= 233472 && NT <= 512) ? 2 : 1;
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, (MINB > 1 && MODE == COL_UPDATE) ? 1 : 3>;
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, (MINB > 1 && MODE == COL_UPDATE) ? 1 : 3, PP>;
   if constexpr (Cfg::STAGES < 1 || (NARROW && MINB < 2) ||
                 (OPS >= OPS_COMPUTED && MODEL == MK_TUNGSTEN)) {
     return -1;
   } else {
     if (L.seg[0].ncols % W != 0 || L.seg[0].col_stride != 1) return -1;
-    auto k = col_tma_kernel<Real, N, W, MODE, DIR, MODEL, INV, OPS, MINB>;
+    auto k = col_tma_kernel<Real, N, W, MODE, DIR, MODEL, INV, OPS, MINB, PP>;
     static int occ = 0;
     if (!occ) {
       cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
@@ -649,11 +649,13 @@ static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
       rc = L.rad_ops    ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_RADIAL, false>(L, s)
            : L.computed ? (L.narrow       ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, true>(L, s)
                            : L.psi_direct ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED_PD, false>(L, s)
+                           : L.pingpong   ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false, true>(L, s)
                                           : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false>(L, s))
                         : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false>(L, s);
     else
-      rc = L.narrow ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, true>(L, s)
-                    : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false>(L, s);
+      rc = L.narrow     ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, true>(L, s)
+           : L.pingpong ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false, true>(L, s)
+                        : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false>(L, s);
     if (rc >= 0) return rc;
   }
   if constexpr (MODE == COL_UPDATE && MODEL != MK_TUNGSTEN) {

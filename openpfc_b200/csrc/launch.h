@@ -68,6 +68,9 @@ struct ColLaunch {
   int psi_direct;
   // COL_PLAIN: half-width tiles (64-byte rows) with two CTAs per SM
   int narrow;
+  // ping-pong FFT exchange buffers (one CTA barrier per exchange; one ring
+  // stage fewer): COL_PLAIN and the computed-operator update
+  int pingpong;
   int axis;            // 1 = y, 2 = z
   unsigned int *flag;  // bit 1: a bounded wait expired
   int num_sms;

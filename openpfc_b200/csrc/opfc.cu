@@ -36,7 +36,7 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 3, kVarX = 3, kVarZ = 7;  // kernel variants per pass (opfc_autotune)
+constexpr int kVarY = 4, kVarX = 3, kVarZ = 8;  // kernel variants per pass (opfc_autotune)
 
 bool supported_len(int n) {
   static const int ok[] = {1, 2, 4, 8, 16, 24, 32, 40, 48, 64, 80, 96, 128, 256, 512, 1024};
@@ -126,14 +126,16 @@ struct opfc_handle {
 
   bool use_tma = true;  // TMA-fed column passes (OPFC_NO_TMA=1 disables)
   // kernel variants per pass, chosen by the autotuner (see opfc_autotune):
-  // var_y: 0 pipelined, 1 direct, 2 pipelined narrow tiles (two CTAs per SM);
+  // var_y: 0 pipelined, 1 direct, 2 pipelined narrow tiles (two CTAs per SM),
+  //        3 pipelined with ping-pong exchange buffers;
   // var_x: 0 pipelined (warp-square kernel where it applies), 1 direct,
   //        2 pipelined without the warp-square kernel;
   // var_z: 0 pipelined with streamed tables, 1 pipelined with radial tables,
   //        2 direct with streamed tables, 3 pipelined with computed operators,
   //        4 direct with computed operators, 5 pipelined with computed operators
   //        and two CTAs per SM, 6 pipelined A with psi_hat prefetched into
-  //        registers and computed operators (3-6: PLAIN and FILTERED)
+  //        registers and computed operators, 7 as 3 with ping-pong exchange
+  //        buffers (3-7: PLAIN and FILTERED)
   int var_y = 0, var_x = 0, var_z = 0;
   int num_sms = 148;
   struct Tmap {
@@ -300,6 +302,7 @@ int col_plain(opfc_handle *h, int axis, int dir, const void *in0, void *out0,
   L.tw = axis == 1 ? h->tw_y : h->tw_z;
   L.axis = axis;
   L.narrow = h->var_y == 2;
+  L.pingpong = h->var_y == 3;
   const int W = tma_col_width(L.N, 2 * (int)h->rsz, COL_PLAIN, L.narrow);
   if (h->use_tma && h->var_y != 1 && L.N > 1 && h->M % W == 0) {
     L.tmap[0] = tmap_for(h, in0, axis, W, false);
@@ -468,6 +471,7 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.computed = h->var_z >= 3 && model != OPFC_MODEL_TUNGSTEN;
     Z.narrow = h->var_z == 5;
     Z.psi_direct = h->var_z == 6;
+    Z.pingpong = h->var_z == 7;
     Z.rad_M = h->M;
     Z.rad_n1 = h->n1;
     Z.rad_n2 = h->n2;
