@@ -153,17 +153,15 @@ const char *opfc_step_kernel_name(int k);
  * where M = R^2 or 2 R^2) | 1 direct | 2 pipelined without it; z update:
  * 0 pipelined with streamed tables | 1 pipelined with radial tables (isotropic
  * grids) | 2 direct with streamed tables | 3 pipelined with operators computed
- * from k^2 | 4 direct with computed operators | 5 pipelined with computed
- * operators, one stage and two CTAs per SM | 6 pipelined A tiles with psi_hat
- * prefetched into registers and computed operators | 7 as 3 with ping-pong
- * exchange buffers (3-7: PLAIN and FILTERED);
+ * from k^2 | 4 direct with computed operators | 5 as 3 with ping-pong exchange
+ * buffers (3-5: PLAIN and FILTERED);
  * 3 warm-up + 10 timed launches each), keeps the fastest and caches it per
  * device; opfc_initialize applies cached choices.  ms (OPFC_AUTOTUNE_SLOTS
  * doubles, may be NULL) receives the mean milliseconds per launch of
- * y0 y1 y2 y3 x0 x1 x2 z0 z1 z2 z3 z4 z5 z6 z7 (-1 if not applicable).  Call after
+ * y0 y1 y2 y3 x0 x1 x2 z0 z1 z2 z3 z4 z5 (-1 if not applicable).  Call after
  * opfc_initialize; the passes run in place, so set the field afterwards.
  * opfc_variants reports the chosen (y, x, z) variants. */
-#define OPFC_AUTOTUNE_SLOTS 15
+#define OPFC_AUTOTUNE_SLOTS 13
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 

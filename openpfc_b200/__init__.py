@@ -211,8 +211,7 @@ class _ModelBase(_Handle):
         """Time every kernel variant of each pass, keep the fastest (cached per
         device); returns ms per launch by variant.  Set the field afterwards."""
         names = ["y.pipelined", "y.direct", "y.narrow", "y.pingpong", "x.pipelined", "x.direct", "x.no_square",
-                 "z.tables", "z.radial", "z.direct", "z.computed", "z.direct_computed", "z.computed_2cta",
-                 "z.computed_psi_direct", "z.computed_pingpong"]
+                 "z.tables", "z.radial", "z.direct", "z.computed", "z.direct_computed", "z.computed_pingpong"]
         ms = (ctypes.c_double * len(names))()
         _check(self._h, lib().opfc_autotune(self._h, ms))
         return dict(zip(names, list(ms)))

@@ -85,9 +85,8 @@ struct TmaCfg {
   static constexpr size_t TILE_R = size_t(N) * W * sizeof(Real);
   // radial operators come from an L2-resident table and computed operators
   // from k^2: only the per-mode tables are staged
-  // (OPS 3: psi_hat is not staged either)
   static constexpr size_t STAGE =
-      TILE_C + (UPD ? (OPS == 3 ? 0 : TILE_C) + (OPS != 0 ? 0 : 2 * TILE_R + (CHI ? TILE_R : 0)) : 0);
+      TILE_C + (UPD ? TILE_C + (OPS != 0 ? 0 : 2 * TILE_R + (CHI ? TILE_R : 0)) : 0);
   static constexpr size_t TW = align128(size_t(N) * sizeof(C));
   // PP: a second FFT exchange buffer (ping-pong with the landed tile)
   static constexpr size_t XB = PP ? align128(TILE_C) : 0;
@@ -135,12 +134,10 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
                    const __grid_constant__ CUtensorMap m2, const __grid_constant__ CUtensorMap m3,
                    const __grid_constant__ CUtensorMap m4, const ColArgs<Real> a, const int axis,
                    unsigned *flag) {
-  // two CTAs per SM for the update: one stage each
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, (MINB > 1 && MODE == COL_UPDATE) ? 1 : 3, PP>;
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, 3, PP>;
   using C = typename Cx<Real>::T;
   constexpr bool RADIAL = OPS == 1;
-  constexpr bool COMPUTED = OPS == 2 || OPS == 3;
-  constexpr bool PD = OPS == 3;  // psi_hat straight into registers
+  constexpr bool COMPUTED = OPS == 2;
   constexpr int E = Plan<N>::E;
   constexpr int T = N / E;
   constexpr int NT = W * T;
@@ -164,7 +161,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
   __syncthreads();
   // the update's two transforms per tile take their stage twiddles from
   // registers when few enough (loaded once: they depend only on j)
-  constexpr bool TWR = UPD && MINB == 1 && TwReg<C, N>::CNT > 0 && TwReg<C, N>::CNT <= 16;
+  constexpr bool TWR = UPD && TwReg<C, N>::CNT > 0 && TwReg<C, N>::CNT <= 16;
   TwReg<C, N> twr;
   if constexpr (TWR) twr.load(j, tw);
 
@@ -186,7 +183,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
       tma_load_3d(st + offc, min, &bars[s], ti * W * 2, y, z);
       if constexpr (UPD) {
         const size_t offr = size_t(b) * Cfg::RB * W * sizeof(Real);
-        if constexpr (!PD) tma_load_3d(st + Cfg::TILE_C + offc, &m1, &bars[s], ti * W * 2, y, z);
+        tma_load_3d(st + Cfg::TILE_C + offc, &m1, &bars[s], ti * W * 2, y, z);
         if constexpr (OPS != 0) continue;
         tma_load_3d(st + 2 * Cfg::TILE_C + offr, &m2, &bars[s], ti * W, y, z);
         tma_load_3d(st + 2 * Cfg::TILE_C + Cfg::TILE_R + offr, &m3, &bars[s], ti * W, y, z);
@@ -237,14 +234,6 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
       // radial operators: gather from L2 before the transform so the loads
       // overlap it (z pass: kx = column, ky = outer index, kz = p)
       Real rla[RADIAL ? E : 1], rlb[RADIAL ? E : 1], rch[RADIAL && Cfg::CHI ? E : 1];
-      // PD: the state of this tile straight from HBM into registers, in flight
-      // during the forward transform
-      C pp[PD ? E : 1];
-      if constexpr (PD) {
-        const C *gph = reinterpret_cast<const C *>(a.psi_hat);
-#pragma unroll
-        for (int m = 0; m < E; ++m) pp[m] = gph[base + (long long)(j + T * m) * fs];
-      }
       if constexpr (RADIAL) {
 #pragma unroll
         for (int m = 0; m < E; ++m) {
@@ -263,11 +252,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
 #pragma unroll
       for (int m = 0; m < E; ++m) {
         const int e = (j + T * m) * W + c;
-        C p;
-        if constexpr (PD)
-          p = pp[m];
-        else
-          p = tpsi[e];
+        const C p = tpsi[e];
         Real la, lb, ch = Real(1);
         if constexpr (RADIAL) {
           la = rla[m];

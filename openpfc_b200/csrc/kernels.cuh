@@ -40,8 +40,7 @@ template <typename Real> struct ColArgs {
 };
 
 // Operator selection of the fused z update.
-// OPS_COMPUTED_PD: computed operators, psi_hat prefetched into registers.
-enum OpsKind { OPS_TABLES = 0, OPS_RADIAL = 1, OPS_COMPUTED = 2, OPS_COMPUTED_PD = 3 };
+enum OpsKind { OPS_TABLES = 0, OPS_RADIAL = 1, OPS_COMPUTED = 2 };
 
 // Plain-PFC operators of mode (kx, ky, kz) (kx unfolded, ky / kz folded), in
 // the compute precision (10_complete_pfc_model.cpp:189-207, kspace.hpp:97-103):
@@ -81,8 +80,7 @@ namespace opfc {
 // column pass: batched FFT along a strided axis (y or z), optional ETD update
 // ---------------------------------------------------------------------------
 template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS>
-__global__ void __launch_bounds__(Width<Real>::W *(N / Plan<N>::E))
-    col_kernel(const ColArgs<Real> a) {
+__global__ void __launch_bounds__(Width<Real>::W *(N / Plan<N>::E)) col_kernel(const ColArgs<Real> a) {
   using C = typename Cx<Real>::T;
   constexpr int W = Width<Real>::W;
   constexpr int E = Plan<N>::E;
@@ -605,16 +603,14 @@ static int launch_col_direct(const ColLaunch &L, cudaStream_t s) {
 template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS, bool NARROW, bool PP = false>
 static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
   using C = typename Cx<Real>::T;
-  constexpr int W = tma_col_width(N, (int)sizeof(C), MODE, NARROW, OPS == OPS_COMPUTED_PD);
+  constexpr int W = tma_col_width(N, (int)sizeof(C), MODE, NARROW);
   constexpr int NT = W * (N / Plan<N>::E);
-  // NARROW: two CTAs per SM when their shared memory fits and each has at most
-  // 512 threads (64 registers per thread); plain transforms take half-width
-  // tiles, the update keeps its width with one stage per CTA
-  using Cfg2 = TmaCfg<Real, N, W, MODE, MODEL, OPS, MODE == COL_UPDATE ? 1 : 3, PP>;
-  constexpr int MINB = (NARROW && Cfg2::STAGES >= 1 && 2 * (Cfg2::SMEM + 1024) <= 233472 && NT <= 512) ? 2 : 1;
-  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, (MINB > 1 && MODE == COL_UPDATE) ? 1 : 3, PP>;
+  // NARROW (plain transforms): half-width tiles, two CTAs per SM when their
+  // shared memory fits and each has at most 512 threads (64 registers per thread)
+  using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, 3, PP>;
+  constexpr int MINB = (NARROW && MODE == COL_PLAIN && 2 * (Cfg::SMEM + 1024) <= 233472 && NT <= 512) ? 2 : 1;
   if constexpr (Cfg::STAGES < 1 || (NARROW && MINB < 2) ||
-                (OPS >= OPS_COMPUTED && MODEL == MK_TUNGSTEN)) {
+                (OPS == OPS_COMPUTED && MODEL == MK_TUNGSTEN)) {
     return -1;
   } else {
     if (L.seg[0].ncols % W != 0 || L.seg[0].col_stride != 1) return -1;
@@ -647,10 +643,8 @@ static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
     int rc;
     if constexpr (MODE == COL_UPDATE)
       rc = L.rad_ops    ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_RADIAL, false>(L, s)
-           : L.computed ? (L.narrow       ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, true>(L, s)
-                           : L.psi_direct ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED_PD, false>(L, s)
-                           : L.pingpong   ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false, true>(L, s)
-                                          : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false>(L, s))
+           : L.computed ? (L.pingpong ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false, true>(L, s)
+                                      : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false>(L, s))
                         : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false>(L, s);
     else
       rc = L.narrow     ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, true>(L, s)

@@ -63,9 +63,6 @@ struct ColLaunch {
   // op_chi = 1 / (2 alpha^2) of the filter (FILTERED).  Uses rad_M/n1/n2.
   int computed;
   double kf[3], op_r, op_dt, op_chi;
-  // COL_UPDATE with computed operators: psi_hat read straight into registers
-  // (prefetched before the forward transform) instead of staged by TMA
-  int psi_direct;
   // COL_PLAIN: half-width tiles (64-byte rows) with two CTAs per SM
   int narrow;
   // ping-pong FFT exchange buffers (one CTA barrier per exchange; one ring
@@ -80,11 +77,9 @@ struct ColLaunch {
 // transforms (64-byte rows and half the tile for the narrow variant) and 64-byte
 // rows for the fused update (which stages psi_hat and the tables too), capped so
 // one tile stays near 64 KB / 32 KB.  Host and device use this one definition.
-// psi_direct: the update stages only A (psi_hat goes straight to registers), so
-// its tile may grow to 64 KB.
-constexpr int tma_col_width(int N, int csize, int mode, bool narrow = false, bool psi_direct = false) {
+constexpr int tma_col_width(int N, int csize, int mode, bool narrow = false) {
   int w = (mode == COL_PLAIN && !narrow ? 128 : 64) / csize;
-  const int cap = (mode == COL_PLAIN && !narrow ? 65536 : (psi_direct ? 65536 : 32768)) / (N * csize);
+  const int cap = (mode == COL_PLAIN && !narrow ? 65536 : 32768) / (N * csize);
   if (cap < w) w = cap;
   return w < 4 ? 4 : w;
 }

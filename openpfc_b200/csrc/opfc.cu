@@ -36,7 +36,7 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 4, kVarX = 3, kVarZ = 8;  // kernel variants per pass (opfc_autotune)
+constexpr int kVarY = 4, kVarX = 3, kVarZ = 6;  // kernel variants per pass (opfc_autotune)
 
 bool supported_len(int n) {
   static const int ok[] = {1, 2, 4, 8, 16, 24, 32, 40, 48, 64, 80, 96, 128, 256, 512, 1024};
@@ -132,10 +132,8 @@ struct opfc_handle {
   //        2 pipelined without the warp-square kernel;
   // var_z: 0 pipelined with streamed tables, 1 pipelined with radial tables,
   //        2 direct with streamed tables, 3 pipelined with computed operators,
-  //        4 direct with computed operators, 5 pipelined with computed operators
-  //        and two CTAs per SM, 6 pipelined A with psi_hat prefetched into
-  //        registers and computed operators, 7 as 3 with ping-pong exchange
-  //        buffers (3-7: PLAIN and FILTERED)
+  //        4 direct with computed operators, 5 as 3 with ping-pong exchange
+  //        buffers (3-5: PLAIN and FILTERED)
   int var_y = 0, var_x = 0, var_z = 0;
   int num_sms = 148;
   struct Tmap {
@@ -469,9 +467,7 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.axis = 2;
     // computed operators (variants 3, 4): PLAIN and FILTERED models
     Z.computed = h->var_z >= 3 && model != OPFC_MODEL_TUNGSTEN;
-    Z.narrow = h->var_z == 5;
-    Z.psi_direct = h->var_z == 6;
-    Z.pingpong = h->var_z == 7;
+    Z.pingpong = h->var_z == 5;
     Z.rad_M = h->M;
     Z.rad_n1 = h->n1;
     Z.rad_n2 = h->n2;
@@ -480,12 +476,12 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.op_r = h->desc.r;
     Z.op_dt = h->dt;
     Z.op_chi = model == OPFC_MODEL_FILTERED ? 1.0 / (2.0 * h->desc.filter_alpha * h->desc.filter_alpha) : 0.0;
-    const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE, false, Z.psi_direct != 0);
+    const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE);
     if (h->use_tma && h->var_z != 2 && h->var_z != 4 && Z.N > 1 && h->M % W == 0) {
       Z.tmap[0] = tmap_for(h, h->work_a, 2, W, false);
       Z.tmap[1] = tmap_for(h, h->psi_hat, 2, W, false);
       if (Z.computed) {
-        if (!Z.tmap[1]) Z.tmap[0] = nullptr;  // (psi_direct: m1 is passed but not read)
+        if (!Z.tmap[1]) Z.tmap[0] = nullptr;
       } else if (h->rad_ops && h->var_z == 1) {
         // isotropic grid: operators from the L2-resident radial tables
         Z.rad_ops = h->rad_ops;

@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 PI4 = [math.pi / 4] * 3
 
 
-@pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "psi_direct", "pingpong"])
+@pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "pingpong"])
 def path(request, monkeypatch):
     """tma: pipelined kernels streaming the per-mode tables (default);
     tma_radial: the z update reading radial operator tables (OPFC_Z_VARIANT=1,
@@ -24,10 +24,8 @@ def path(request, monkeypatch):
     (OPFC_Z_VARIANT=3), half-width y tiles (OPFC_Y_VARIANT=2) and the x pass
     without the warp-square kernel (OPFC_X_VARIANT=2);
     direct_computed: direct z update computing its operators (OPFC_Z_VARIANT=4);
-    psi_direct: pipelined z update with psi_hat prefetched into registers
-    (OPFC_Z_VARIANT=6);
     pingpong: ping-pong FFT exchange buffers in the y pass and the computed
-    z update (OPFC_Y_VARIANT=3, OPFC_Z_VARIANT=7).
+    z update (OPFC_Y_VARIANT=3, OPFC_Z_VARIANT=5).
     The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
@@ -44,11 +42,9 @@ def path(request, monkeypatch):
         monkeypatch.setenv("OPFC_X_VARIANT", "2")
     elif request.param == "direct_computed":
         monkeypatch.setenv("OPFC_Z_VARIANT", "4")
-    elif request.param == "psi_direct":
-        monkeypatch.setenv("OPFC_Z_VARIANT", "6")
     elif request.param == "pingpong":
         monkeypatch.setenv("OPFC_Y_VARIANT", "3")
-        monkeypatch.setenv("OPFC_Z_VARIANT", "7")
+        monkeypatch.setenv("OPFC_Z_VARIANT", "5")
     return request.param
 
 
