@@ -34,6 +34,7 @@ extern "C" {
 #define OPFC_ERR_TIMEOUT (-5)     /* bounded device wait expired                */
 #define OPFC_ERR_OOM (-6)         /* device allocation failed                   */
 #define OPFC_ERR_STATE (-7)       /* call out of order (e.g. step before init)  */
+#define OPFC_ERR_IO (-8)          /* file could not be opened / written         */
 
 /* precision of the bulk arithmetic */
 #define OPFC_FP32 0
@@ -218,6 +219,45 @@ int opfc_ic_seed(double *psi, const int n[3], const double dx[3], const double o
                  const double center[3], double radius, double rho, double amp, int outside_zero);
 int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, double noise,
                   int nseeds, double radius_cells, double amp, uint64_t seed);
+
+/* On-disk formats of the reference's writers and readers (one process owns
+ * the whole grid; no MPI).
+ * opfc_format_filename: pfc::utils::format_with_number
+ *   (include/openpfc/frontend/utils/utils.hpp:96-139): a pattern without '%' is
+ *   returned as is; otherwise exactly one "%[-+ 0][*][width]d" and no other '%'
+ *   (else OPFC_ERR_ARG); out_len too small -> OPFC_ERR_SIZE.
+ * opfc_write_binary: psi as raw native FP64, x fastest, no header, file named
+ *   format_with_number(pattern, increment) and truncated first
+ *   (BinaryWriter::write(increment, RealField),
+ *   include/openpfc/frontend/io/binary_writer.hpp).
+ * opfc_write_binary_hat: psi_hat in the reference layout ((N0/2+1) x N1 x N2,
+ *   interleaved re, im FP64), BinaryWriter::write(increment, ComplexField).
+ * opfc_read_binary: such a raw FP64 psi file -> the state, as opfc_set_psi
+ *   (FileReader::apply, include/openpfc/kernel/simulation/initial_conditions/
+ *   file_reader.hpp, via BinaryReader::read); a short file -> OPFC_ERR_SIZE.
+ * opfc_write_vti: psi as VTK XML ImageData, one Float64 point array appended
+ *   raw with a UInt64 length prefix, Origin / Spacing from the descriptor,
+ *   array name field_name (NULL: "Field") (VTKWriter::write,
+ *   src/openpfc/frontend/io/vtk_writer.cpp:70-108,166-225).
+ * File errors -> OPFC_ERR_IO with the message in opfc_last_error. */
+int opfc_format_filename(const char *pattern, int increment, char *out, size_t out_len);
+int opfc_write_binary(opfc_handle *h, const char *pattern, int increment);
+int opfc_write_binary_hat(opfc_handle *h, const char *pattern, int increment);
+int opfc_read_binary(opfc_handle *h, const char *filename);
+int opfc_write_vti(opfc_handle *h, const char *pattern, int increment, const char *field_name);
+/* The same formats for host arrays and one process's box of a global grid
+ * (x fastest; box = local extent at offset, as set_domain(global, local,
+ * offset) of the reference's writers): opfc_write_raw truncates `filename`
+ * and writes the box of `ncomp` (1 real, 2 complex) doubles per point at its
+ * place in the global array; opfc_read_raw reads such a box (short file ->
+ * OPFC_ERR_SIZE); opfc_write_vti_raw writes one .vti piece.  A box outside
+ * the grid -> OPFC_ERR_ARG. */
+int opfc_write_raw(const char *filename, const int global[3], const int local[3], const int offset[3],
+                   const double *data, int ncomp);
+int opfc_read_raw(const char *filename, const int global[3], const int local[3], const int offset[3],
+                  double *data, int ncomp);
+int opfc_write_vti_raw(const char *filename, const int global[3], const int local[3], const int offset[3],
+                       const double origin[3], const double spacing[3], const char *name, const double *data);
 
 /* Forward R2C transform that allocates nothing (no counterpart in the
  * reference; it is opfc_fft_forward without a handle).  For callers that cannot

@@ -7,6 +7,10 @@
 //   pfc::b200::TungstenB200<T> -- the Tungsten model (cpu/tungsten_model.hpp:123-380,
 //                              cuda/tungsten_model.hpp:80-500)
 //   pfc::b200::PfcB200<T>   -- the plain conserved PFC model (docs/api/examples/10_complete_pfc_model.cpp:62-214)
+//   pfc::b200::BinaryWriter / BinaryReader / VTKWriter / FileReader / format_with_number
+//                           -- the on-disk formats (frontend/io/binary_writer.hpp,
+//                              kernel/simulation/binary_reader.hpp, frontend/io/vtk_writer.hpp,
+//                              initial_conditions/file_reader.hpp, frontend/utils/utils.hpp)
 // Size contracts throw std::invalid_argument, unknown fields std::out_of_range,
 // everything else std::runtime_error (as in the reference).  T selects the
 // device precision (float or double); host fields are std::vector<double>.
@@ -22,6 +26,7 @@
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../openpfc_b200.h"
@@ -227,6 +232,7 @@ template <typename T> class ModelBase {
   size_t get_allocated_memory_bytes() const { return h_ ? opfc_allocated_bytes(h_) : 0; }
   opfc_handle *handle() { return h_; }
   size_t cells() const { return (size_t)n_[0] * n_[1] * n_[2]; }
+  std::array<int, 3> dims() const { return n_; }
 
  protected:
   virtual opfc_desc describe() const = 0;
@@ -316,6 +322,139 @@ template <typename T = double> class PfcB200 : public detail::ModelBase<T> {
 
  private:
   double epsilon_;
+};
+
+// ---------------------------------------------------------------------------
+// On-disk formats: host-side mirrors of the reference's writers and readers
+// for one process (set_domain(global, local, offset) as the MPI versions; the
+// box is written at its place in the global file).  Same file layouts:
+// BinaryWriter / BinaryReader (frontend/io/binary_writer.hpp,
+// kernel/simulation/binary_reader.hpp), VTKWriter (frontend/io/vtk_writer.hpp),
+// FileReader (kernel/simulation/initial_conditions/file_reader.hpp).
+// ---------------------------------------------------------------------------
+
+/// pfc::utils::format_with_number; throws std::invalid_argument on a bad pattern.
+inline std::string format_with_number(const std::string &pattern, int increment) {
+  std::vector<char> out(pattern.size() + 64);
+  const int rc = opfc_format_filename(pattern.c_str(), increment, out.data(), out.size());
+  if (rc == OPFC_ERR_ARG) throw std::invalid_argument("format_with_number: invalid filename pattern '" + pattern + "'");
+  check(rc, "format_with_number");
+  return std::string(out.data());
+}
+
+class DomainIO {
+ public:
+  explicit DomainIO(std::string filename) : filename_(std::move(filename)) {}
+  void set_domain(const std::array<int, 3> &global, const std::array<int, 3> &local,
+                  const std::array<int, 3> &offset) {
+    for (int a = 0; a < 3; ++a)
+      if (global[a] < 1 || local[a] < 1 || offset[a] < 0 || offset[a] + local[a] > global[a])
+        throw std::invalid_argument("set_domain: local box outside the global box");
+    global_ = global;
+    local_ = local;
+    offset_ = offset;
+    valid_ = true;
+  }
+
+ protected:
+  size_t expect(const char *who, size_t got) const {
+    if (!valid_) throw std::runtime_error(std::string(who) + ": set_domain() was not called");
+    const size_t n = (size_t)local_[0] * local_[1] * local_[2];
+    if (got != n)
+      throw std::runtime_error(std::string(who) + ": buffer size mismatch (expected " + std::to_string(n) +
+                               " elements from set_domain, got " + std::to_string(got) + ")");
+    return n;
+  }
+  std::string filename_;
+  std::array<int, 3> global_{}, local_{}, offset_{};
+  bool valid_ = false;
+};
+
+/// Raw native doubles of the global array, x fastest, no header.
+class BinaryWriter : public DomainIO {
+ public:
+  using DomainIO::DomainIO;
+  void write(int increment, const std::vector<double> &data) {
+    expect("BinaryWriter::write", data.size());
+    const std::string fn = format_with_number(filename_, increment);
+    check(opfc_write_raw(fn.c_str(), global_.data(), local_.data(), offset_.data(), data.data(), 1),
+          "BinaryWriter::write", fn.c_str());
+  }
+  void write(int increment, const std::vector<std::complex<double>> &data) {
+    expect("BinaryWriter::write", data.size());
+    const std::string fn = format_with_number(filename_, increment);
+    check(opfc_write_raw(fn.c_str(), global_.data(), local_.data(), offset_.data(),
+                         reinterpret_cast<const double *>(data.data()), 2),
+          "BinaryWriter::write", fn.c_str());
+  }
+};
+
+class BinaryReader : public DomainIO {
+ public:
+  BinaryReader() : DomainIO("") {}
+  void read(const std::string &filename, std::vector<double> &data) {
+    expect("BinaryReader::read", data.size());
+    check(opfc_read_raw(filename.c_str(), global_.data(), local_.data(), offset_.data(), data.data(), 1),
+          "BinaryReader::read", filename.c_str());
+  }
+  void read(const std::string &filename, std::vector<std::complex<double>> &data) {
+    expect("BinaryReader::read", data.size());
+    check(opfc_read_raw(filename.c_str(), global_.data(), local_.data(), offset_.data(),
+                        reinterpret_cast<double *>(data.data()), 2),
+          "BinaryReader::read", filename.c_str());
+  }
+};
+
+/// VTK XML ImageData piece (.vti), Float64 point data appended raw; a complex
+/// field is written as its magnitude.
+class VTKWriter : public DomainIO {
+ public:
+  using DomainIO::DomainIO;
+  void set_origin(const std::array<double, 3> &o) { origin_ = o; }
+  void set_spacing(const std::array<double, 3> &s) {
+    for (double v : s)
+      if (!(v > 0)) throw std::invalid_argument("VTKWriter::set_spacing: spacing must be positive");
+    spacing_ = s;
+  }
+  void set_field_name(const std::string &name) { name_ = name; }
+  void write(int increment, const std::vector<double> &data) {
+    expect("VTKWriter::write", data.size());
+    const std::string fn = format_with_number(filename_, increment);
+    check(opfc_write_vti_raw(fn.c_str(), global_.data(), local_.data(), offset_.data(), origin_.data(),
+                             spacing_.data(), name_.c_str(), data.data()),
+          "VTKWriter::write", fn.c_str());
+  }
+  void write(int increment, const std::vector<std::complex<double>> &data) {
+    std::vector<double> mag(data.size());
+    for (size_t i = 0; i < data.size(); ++i) mag[i] = std::abs(data[i]);
+    write(increment, mag);
+  }
+
+ private:
+  std::array<double, 3> origin_{0, 0, 0}, spacing_{1, 1, 1};
+  std::string name_ = "Field";
+};
+
+/// Initial condition from a raw FP64 file (FieldModifier::apply).
+class FileReader {
+ public:
+  FileReader() = default;
+  explicit FileReader(std::string filename) : filename_(std::move(filename)) {}
+  void set_filename(std::string filename) { filename_ = std::move(filename); }
+  const std::string &get_filename() const { return filename_; }
+  template <typename Model> void apply(Model &m, double /*time*/) {
+    std::vector<double> &psi = m.get_real_field("psi");
+    BinaryReader r;
+    r.set_domain(m.dims(), m.dims(), {0, 0, 0});
+    try {
+      r.read(filename_, psi);
+    } catch (const std::exception &ex) {
+      throw std::runtime_error("FileReader failed to read \"" + filename_ + "\" into field \"psi\": " + ex.what());
+    }
+  }
+
+ private:
+  std::string filename_;
 };
 
 }  // namespace b200

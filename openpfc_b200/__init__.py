@@ -204,6 +204,23 @@ class _ModelBase(_Handle):
         _check(self._h, lib().opfc_free_energy(self._h, ctypes.byref(v)))
         return v.value
 
+    # on-disk formats of the reference (BinaryWriter / FileReader / VTKWriter)
+    def write_binary(self, pattern: str, increment: int = 0):
+        """psi as raw FP64, x fastest, no header; file format_with_number(pattern, increment)."""
+        _check(self._h, lib().opfc_write_binary(self._h, pattern.encode(), int(increment)))
+
+    def write_binary_hat(self, pattern: str, increment: int = 0):
+        """psi_hat, reference layout, raw interleaved complex FP64."""
+        _check(self._h, lib().opfc_write_binary_hat(self._h, pattern.encode(), int(increment)))
+
+    def read_binary(self, filename: str):
+        """Set the state from a raw FP64 psi file (FileReader initial condition)."""
+        _check(self._h, lib().opfc_read_binary(self._h, filename.encode()))
+
+    def write_vti(self, pattern: str, increment: int = 0, field_name: str = "Field"):
+        """psi as VTK XML ImageData (.vti), Float64, appended raw."""
+        _check(self._h, lib().opfc_write_vti(self._h, pattern.encode(), int(increment), field_name.encode()))
+
     def kernels_per_step(self) -> int:
         return int(lib().opfc_kernels_per_step(self._h))
 
@@ -299,6 +316,22 @@ class TungstenB200(_ModelBase):
         if params is not None:
             d.tungsten = params
         super().__init__(d)
+
+
+# ---------------------------------------------------------------------------
+# file names (pfc::utils::format_with_number)
+# ---------------------------------------------------------------------------
+
+def format_with_number(pattern: str, increment: int) -> str:
+    """A pattern without '%' unchanged; else exactly one %d (flags -+ 0, width)
+    replaced by the increment; anything else raises ValueError."""
+    out = ctypes.create_string_buffer(4096)
+    rc = lib().opfc_format_filename(pattern.encode(), int(increment), out, len(out))
+    if rc == -1:
+        raise ValueError(f"invalid filename pattern {pattern!r}")
+    if rc != 0:
+        raise RuntimeError(f"opfc_format_filename failed ({rc})")
+    return out.value.decode()
 
 
 # ---------------------------------------------------------------------------

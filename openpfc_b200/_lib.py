@@ -16,7 +16,7 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "openpfc_b200.h")
 OPFC_OK = 0
 STATUS = {0: "OPFC_OK", -1: "OPFC_ERR_ARG", -2: "OPFC_ERR_SIZE", -3: "OPFC_ERR_CUDA",
           -4: "OPFC_ERR_NONFINITE", -5: "OPFC_ERR_TIMEOUT", -6: "OPFC_ERR_OOM",
-          -7: "OPFC_ERR_STATE"}
+          -7: "OPFC_ERR_STATE", -8: "OPFC_ERR_IO"}
 FP32, FP64 = 0, 1
 MODEL_PLAIN, MODEL_TUNGSTEN, MODEL_FILTERED = 0, 1, 2
 HOST, DEVICE = 0, 1
@@ -106,6 +106,15 @@ def lib():
     L.opfc_ic_seed.argtypes = [dp, ip, dp, dp, dp, cd, cd, cd, ci]
     L.opfc_ic_seeds.argtypes = [dp, ip, dp, cd, cd, ci, cd, cd, ctypes.c_uint64]
     L.opfc_fft_forward_noalloc.argtypes = [vp, vp, ip, ci, vp]
+    cp = ctypes.c_char_p
+    L.opfc_format_filename.argtypes = [cp, ci, ctypes.c_char_p, sz]
+    L.opfc_write_binary.argtypes = [H, cp, ci]
+    L.opfc_write_binary_hat.argtypes = [H, cp, ci]
+    L.opfc_read_binary.argtypes = [H, cp]
+    L.opfc_write_vti.argtypes = [H, cp, ci, cp]
+    L.opfc_write_raw.argtypes = [cp, ip, ip, ip, dp, ci]
+    L.opfc_read_raw.argtypes = [cp, ip, ip, ip, dp, ci]
+    L.opfc_write_vti_raw.argtypes = [cp, ip, ip, ip, dp, dp, cp, dp]
     L.opfc_ensemble_create.argtypes = [ci, ctypes.POINTER(Desc), ctypes.POINTER(H)]
     L.opfc_ensemble_destroy.argtypes = [H]
     L.opfc_ensemble_last_error.argtypes = [H]

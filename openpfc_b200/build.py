@@ -21,9 +21,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libopenpfc_b200.so")
-SOURCES = ["kernels_f32.cu", "kernels_f64.cu", "opfc.cu", "noalloc.cu", "ensemble.cu"]
+SOURCES = ["kernels_f32.cu", "kernels_f64.cu", "opfc.cu", "noalloc.cu", "ensemble.cu", "io.cu"]
 HEADERS = ["fft_core.cuh", "kernels.cuh", "launch.h", "col_tma.cuh", "x_tma.cuh", "x_sq.cuh", "twiddle.h",
-           "ensemble.cuh", "autotune.h"]
+           "ensemble.cuh", "autotune.h", "io.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",

@@ -28,6 +28,7 @@
 #include "launch.h"
 #include "twiddle.h"
 #include "autotune.h"
+#include "io.h"
 
 using namespace opfc;
 
@@ -751,11 +752,65 @@ const char *opfc_status_string(int s) {
     case OPFC_ERR_TIMEOUT: return "device wait timed out";
     case OPFC_ERR_OOM: return "device out of memory";
     case OPFC_ERR_STATE: return "call out of order";
+    case OPFC_ERR_IO: return "file I/O failed";
   }
   return "unknown status";
 }
 
 const char *opfc_last_error(const opfc_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+// ---------------------------------------------------------------------------
+// on-disk formats (io.h): the field goes through the host in FP64
+// ---------------------------------------------------------------------------
+static int io_fail(opfc_handle *h, int rc, const std::string &msg) { return fail(h, rc, "%s", msg.c_str()); }
+
+int opfc_write_binary(opfc_handle *h, const char *pattern, int increment) {
+  if (!h) return OPFC_ERR_ARG;
+  std::string fn, err;
+  int rc;
+  if ((rc = io::format_with_number(pattern, increment, fn, err))) return io_fail(h, rc, err);
+  std::vector<double> psi(h->nr);
+  if ((rc = opfc_get_psi(h, psi.data(), h->nr, OPFC_F64, OPFC_HOST))) return rc;
+  const int n[3] = {h->n0, h->n1, h->n2}, zero[3] = {0, 0, 0};
+  if ((rc = io::write_box(fn, n, n, zero, psi.data(), 1, err))) return io_fail(h, rc, err);
+  return OPFC_OK;
+}
+
+int opfc_write_binary_hat(opfc_handle *h, const char *pattern, int increment) {
+  if (!h) return OPFC_ERR_ARG;
+  std::string fn, err;
+  int rc;
+  if ((rc = io::format_with_number(pattern, increment, fn, err))) return io_fail(h, rc, err);
+  std::vector<double> hat(2 * h->nc);
+  if ((rc = opfc_get_psi_hat(h, hat.data(), h->nc, OPFC_F64, OPFC_HOST))) return rc;
+  const int n[3] = {h->n0 / 2 + 1, h->n1, h->n2}, zero[3] = {0, 0, 0};
+  if ((rc = io::write_box(fn, n, n, zero, hat.data(), 2, err))) return io_fail(h, rc, err);
+  return OPFC_OK;
+}
+
+int opfc_read_binary(opfc_handle *h, const char *filename) {
+  if (!h) return OPFC_ERR_ARG;
+  if (!filename) return fail(h, OPFC_ERR_ARG, "null file name");
+  std::string err;
+  std::vector<double> psi(h->nr);
+  const int n[3] = {h->n0, h->n1, h->n2}, zero[3] = {0, 0, 0};
+  int rc;
+  if ((rc = io::read_box(filename, n, n, zero, psi.data(), 1, err))) return io_fail(h, rc, err);
+  return opfc_set_psi(h, psi.data(), h->nr, OPFC_F64, OPFC_HOST);
+}
+
+int opfc_write_vti(opfc_handle *h, const char *pattern, int increment, const char *field_name) {
+  if (!h) return OPFC_ERR_ARG;
+  std::string fn, err;
+  int rc;
+  if ((rc = io::format_with_number(pattern, increment, fn, err))) return io_fail(h, rc, err);
+  std::vector<double> psi(h->nr);
+  if ((rc = opfc_get_psi(h, psi.data(), h->nr, OPFC_F64, OPFC_HOST))) return rc;
+  const int n[3] = {h->n0, h->n1, h->n2}, zero[3] = {0, 0, 0};
+  if ((rc = io::write_vti(fn, n, n, zero, h->desc.origin, h->desc.dx, field_name, psi.data(), err)))
+    return io_fail(h, rc, err);
+  return OPFC_OK;
+}
 
 int opfc_destroy(opfc_handle *h) {
   if (!h) return OPFC_ERR_ARG;
