@@ -44,6 +44,7 @@ extern "C" {
 #define OPFC_MODEL_PLAIN 0     /* conserved PFC, docs/api/examples/10_complete_pfc_model.cpp:121-213 */
 #define OPFC_MODEL_TUNGSTEN 1  /* Tungsten ETD, apps/tungsten/include/tungsten/cpu/tungsten_model.hpp:306-366 */
 #define OPFC_MODEL_FILTERED 2  /* Gaussian mean-field filter + polynomial of psi_MF */
+#define OPFC_MODEL_ALUMINUM 3  /* Aluminum PFC variant, apps/aluminumNew/Aluminum.hpp */
 
 /* where a user pointer lives */
 #define OPFC_HOST 0
@@ -61,6 +62,18 @@ typedef struct opfc_tungsten_params {
   double lambda, stabP, shift_u, shift_s, p2, p3, p4, q20, q21, q30, q31, q40;
 } opfc_tungsten_params;
 
+/* Aluminum PFC parameters: the fields of Aluminum::params
+ * (apps/aluminumNew/Aluminum.hpp:29-82), same names; the reference leaves
+ * unset fields at 0 (opfc_desc_default: all 0, T0 = 1).  The GPU path takes
+ * G_grid = 0 (no moving temperature gradient; G_grid != 0 is refused). */
+typedef struct opfc_aluminum_params {
+  double n0, n_sol, n_vap, T, T0, Bx, T_const, T_max, T_min, G_grid, V_grid, x_initial, m_xpos, alpha,
+      alpha_farTol;
+  int alpha_highOrd;
+  double tau_const, lambda, stabP, shift_u, shift_s, p2, p3, p4, p2_bar, p3_bar, p4_bar, q20, q21, q30, q31,
+      q40, q20_bar, q21_bar, q30_bar, q31_bar, q40_bar, q2_bar, q3_bar, q4_bar, q2_bar_L;
+} opfc_aluminum_params;
+
 typedef struct opfc_desc {
   int n[3];            /* N0 (x, fastest), N1, N2 */
   double dx[3];        /* grid spacing */
@@ -73,6 +86,7 @@ typedef struct opfc_desc {
   opfc_tungsten_params tungsten; /* TUNGSTEN */
   void *stream;        /* cudaStream_t to use, or NULL for a private stream */
   int device;          /* CUDA device ordinal */
+  opfc_aluminum_params aluminum; /* ALUMINUM */
 } opfc_desc;
 
 typedef struct opfc_handle opfc_handle;
@@ -219,6 +233,13 @@ int opfc_ic_seed(double *psi, const int n[3], const double dx[3], const double o
                  const double center[3], double radius, double rho, double amp, int outside_zero);
 int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, double noise,
                   int nseeds, double radius_cells, double amp, uint64_t seed);
+/* opfc_ic_seed_grid_fcc: the Aluminum app's SeedGridFCC (apps/aluminumNew/
+ * SeedGridFCC.hpp, SeedFCC.hpp) on a pre-filled field: Ny x Nz FCC seeds at
+ * x = X0 (+ jitter), rotated at random; positions and angles from
+ * std::mt19937_64(rseed) through std::uniform_real_distribution in the
+ * reference's order (the standard library's mapping, as in the reference). */
+int opfc_ic_seed_grid_fcc(double *psi, const int n[3], const double dx[3], const double origin[3], int Nx, int Ny,
+                          int Nz, double X0, double radius, double amplitude, double rho, double rseed);
 
 /* On-disk formats of the reference's writers and readers (one process owns
  * the whole grid; no MPI).

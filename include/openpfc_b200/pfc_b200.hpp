@@ -285,6 +285,81 @@ template <typename T = double> class TungstenB200 : public detail::ModelBase<T> 
   }
 };
 
+/// Aluminum PFC variant (apps/aluminumNew/Aluminum.hpp): fields "psi",
+/// "default" and "psiMF"; the same setters as Aluminum (set_n0 ... set_q2_bar_L)
+/// on a parameter block that starts at 0 (T0 = 1) like Aluminum::params.  The
+/// moving temperature gradient (G_grid != 0) is refused by initialize().
+template <typename T = double> class AluminumB200 : public detail::ModelBase<T> {
+ public:
+  AluminumB200(std::array<int, 3> n, std::array<double, 3> dx, std::array<double, 3> origin = {}, int device = 0)
+      : detail::ModelBase<T>(n, dx, origin, device) {
+    opfc_desc d;
+    opfc_desc_default(&d);
+    params = d.aluminum;
+    this->fields_["psi"];
+    this->fields_["default"];
+    this->fields_["psiMF"];
+  }
+  opfc_aluminum_params params;
+#define OPFC_ALU(name, type) \
+  void set_##name(type v) { params.name = v; }
+  OPFC_ALU(n0, double)
+  OPFC_ALU(n_sol, double)
+  OPFC_ALU(n_vap, double)
+  OPFC_ALU(T, double)
+  OPFC_ALU(T0, double)
+  OPFC_ALU(Bx, double)
+  OPFC_ALU(T_const, double)
+  OPFC_ALU(T_max, double)
+  OPFC_ALU(T_min, double)
+  OPFC_ALU(G_grid, double)
+  OPFC_ALU(V_grid, double)
+  OPFC_ALU(x_initial, double)
+  OPFC_ALU(m_xpos, double)
+  OPFC_ALU(alpha, double)
+  OPFC_ALU(alpha_farTol, double)
+  OPFC_ALU(alpha_highOrd, int)
+  OPFC_ALU(tau_const, double)
+  OPFC_ALU(lambda, double)
+  OPFC_ALU(stabP, double)
+  OPFC_ALU(shift_u, double)
+  OPFC_ALU(shift_s, double)
+  OPFC_ALU(p2, double)
+  OPFC_ALU(p3, double)
+  OPFC_ALU(p4, double)
+  OPFC_ALU(p2_bar, double)
+  OPFC_ALU(p3_bar, double)
+  OPFC_ALU(p4_bar, double)
+  OPFC_ALU(q20, double)
+  OPFC_ALU(q21, double)
+  OPFC_ALU(q30, double)
+  OPFC_ALU(q31, double)
+  OPFC_ALU(q40, double)
+  OPFC_ALU(q20_bar, double)
+  OPFC_ALU(q21_bar, double)
+  OPFC_ALU(q30_bar, double)
+  OPFC_ALU(q31_bar, double)
+  OPFC_ALU(q40_bar, double)
+  OPFC_ALU(q2_bar, double)
+  OPFC_ALU(q3_bar, double)
+  OPFC_ALU(q4_bar, double)
+  OPFC_ALU(q2_bar_L, double)
+#undef OPFC_ALU
+
+ protected:
+  opfc_desc describe() const override {
+    opfc_desc d = this->base_desc();
+    d.model = OPFC_MODEL_ALUMINUM;
+    d.aluminum = params;
+    return d;
+  }
+  void download_extra() override {
+    this->fields_.at("default") = this->fields_.at("psi");
+    std::vector<double> &mf = this->fields_.at("psiMF");
+    check(opfc_get_psi_mf(this->h_, mf.data(), mf.size(), OPFC_F64, OPFC_HOST), "psiMF");
+  }
+};
+
 /// Plain conserved PFC (10_complete_pfc_model.cpp:62-214): field "density"
 /// (registered name in the example) and "psi".
 template <typename T = double> class PfcB200 : public detail::ModelBase<T> {

@@ -22,10 +22,11 @@ import ctypes
 import numpy as np
 
 from . import _lib
-from ._lib import (DEVICE, F32, F64, FP32, FP64, HOST, MODEL_FILTERED, MODEL_PLAIN,
-                   MODEL_TUNGSTEN, Desc, OpfcError, TungstenParams, default_desc, lib)
+from ._lib import (DEVICE, F32, F64, FP32, FP64, HOST, MODEL_ALUMINUM, MODEL_FILTERED, MODEL_PLAIN,
+                   MODEL_TUNGSTEN, AluminumParams, Desc, OpfcError, TungstenParams, default_desc, lib)
 
-__all__ = ["B200Fft", "PfcB200", "TungstenB200", "FilteredB200", "Desc", "TungstenParams",
+__all__ = ["B200Fft", "PfcB200", "TungstenB200", "FilteredB200", "AluminumB200", "AluminumParams", "Desc",
+           "TungstenParams",
            "OpfcError", "default_desc", "lib", "FP32", "FP64"]
 
 
@@ -318,6 +319,22 @@ class TungstenB200(_ModelBase):
         super().__init__(d)
 
 
+class AluminumB200(_ModelBase):
+    """Aluminum PFC variant (apps/aluminumNew/Aluminum.hpp): Tungsten-form step
+    with the two-Gaussian correlation peak P_F; ``params`` is an AluminumParams
+    (fields the caller leaves unset stay 0, T0 = 1, as in the reference).  The
+    moving temperature gradient (G_grid != 0) is refused by initialize()."""
+
+    def __init__(self, n, dx, params: AluminumParams | None = None, precision: int = FP64,
+                 device: int = 0, origin=None, stream=None):
+        d = default_desc()
+        _geom(d, n, dx, origin, precision, device, stream)
+        d.model = MODEL_ALUMINUM
+        if params is not None:
+            d.aluminum = params
+        super().__init__(d)
+
+
 # ---------------------------------------------------------------------------
 # file names (pfc::utils::format_with_number)
 # ---------------------------------------------------------------------------
@@ -364,6 +381,17 @@ def ic_seed(psi: np.ndarray, dx, origin, center, radius, rho, amp, outside_zero=
     _check(None, lib().opfc_ic_seed(_dp(psi), _i3(n), _d3(dx), _d3(origin), _d3(center), radius,
                                     rho, amp, int(outside_zero)))
     return psi
+
+
+def ic_seed_grid_fcc(psi: np.ndarray, dx, origin, Nx, Ny, Nz, X0, radius, amplitude, rho, rseed) -> np.ndarray:
+    """SeedGridFCC (apps/aluminumNew/SeedGridFCC.hpp) applied to a copy of psi."""
+    out = np.ascontiguousarray(psi, dtype=np.float64).copy()
+    n = (out.shape[2], out.shape[1], out.shape[0])
+    rc = lib().opfc_ic_seed_grid_fcc(_dp(out), _i3(n), _d3(dx), _d3(origin), int(Nx), int(Ny), int(Nz),
+                                     float(X0), float(radius), float(amplitude), float(rho), float(rseed))
+    if rc != 0:
+        raise ValueError(f"opfc_ic_seed_grid_fcc: {rc}")
+    return out
 
 
 def ic_seeds(n, dx, n0, noise, nseeds, radius_cells, amp, seed) -> np.ndarray:

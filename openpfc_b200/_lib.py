@@ -18,7 +18,7 @@ STATUS = {0: "OPFC_OK", -1: "OPFC_ERR_ARG", -2: "OPFC_ERR_SIZE", -3: "OPFC_ERR_C
           -4: "OPFC_ERR_NONFINITE", -5: "OPFC_ERR_TIMEOUT", -6: "OPFC_ERR_OOM",
           -7: "OPFC_ERR_STATE", -8: "OPFC_ERR_IO"}
 FP32, FP64 = 0, 1
-MODEL_PLAIN, MODEL_TUNGSTEN, MODEL_FILTERED = 0, 1, 2
+MODEL_PLAIN, MODEL_TUNGSTEN, MODEL_FILTERED, MODEL_ALUMINUM = 0, 1, 2, 3
 HOST, DEVICE = 0, 1
 F32, F64 = 0, 1
 
@@ -38,6 +38,17 @@ class TungstenParams(ctypes.Structure):
                 ("q40", ctypes.c_double)]
 
 
+class AluminumParams(ctypes.Structure):
+    """Mirror of opfc_aluminum_params (Aluminum::params, apps/aluminumNew/Aluminum.hpp:29-82)."""
+    _fields_ = [(k, ctypes.c_double) for k in
+                ["n0", "n_sol", "n_vap", "T", "T0", "Bx", "T_const", "T_max", "T_min", "G_grid", "V_grid",
+                 "x_initial", "m_xpos", "alpha", "alpha_farTol"]] + [("alpha_highOrd", ctypes.c_int)] + \
+        [(k, ctypes.c_double) for k in
+         ["tau_const", "lambda_", "stabP", "shift_u", "shift_s", "p2", "p3", "p4", "p2_bar", "p3_bar", "p4_bar",
+          "q20", "q21", "q30", "q31", "q40", "q20_bar", "q21_bar", "q30_bar", "q31_bar", "q40_bar", "q2_bar",
+          "q3_bar", "q4_bar", "q2_bar_L"]]
+
+
 class Desc(ctypes.Structure):
     """Mirror of opfc_desc."""
     _fields_ = [("n", ctypes.c_int * 3), ("dx", ctypes.c_double * 3),
@@ -46,7 +57,7 @@ class Desc(ctypes.Structure):
                 ("filter_alpha", ctypes.c_double), ("p2", ctypes.c_double),
                 ("p3", ctypes.c_double), ("p4", ctypes.c_double),
                 ("tungsten", TungstenParams), ("stream", ctypes.c_void_p),
-                ("device", ctypes.c_int)]
+                ("device", ctypes.c_int), ("aluminum", AluminumParams)]
 
 
 class OpfcError(RuntimeError):
@@ -105,6 +116,7 @@ def lib():
     L.opfc_ic_noise.argtypes = [dp, sz, cd, cd, ctypes.c_uint64]
     L.opfc_ic_seed.argtypes = [dp, ip, dp, dp, dp, cd, cd, cd, ci]
     L.opfc_ic_seeds.argtypes = [dp, ip, dp, cd, cd, ci, cd, cd, ctypes.c_uint64]
+    L.opfc_ic_seed_grid_fcc.argtypes = [dp, ip, dp, dp, ci, ci, ci, cd, cd, cd, cd, cd]
     L.opfc_fft_forward_noalloc.argtypes = [vp, vp, ip, ci, vp]
     cp = ctypes.c_char_p
     L.opfc_format_filename.argtypes = [cp, ci, ctypes.c_char_p, sz]

@@ -37,7 +37,9 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 4, kVarX = 3, kVarZ = 6;  // kernel variants per pass (opfc_autotune)
+constexpr int kVarY = 4, kVarX = 3, kVarZ = 6;
+// models with two real fields per step (psi and psi_MF): Tungsten, Aluminum
+inline bool two_field(int model) { return model == OPFC_MODEL_TUNGSTEN || model == OPFC_MODEL_ALUMINUM; }  // kernel variants per pass (opfc_autotune)
 
 bool supported_len(int n) {
   static const int ok[] = {1, 2, 4, 8, 16, 24, 32, 40, 48, 64, 80, 96, 128, 256, 512, 1024};
@@ -363,7 +365,7 @@ double mean_density(const opfc_handle *h) { return h->mass_sum / (double)h->nr; 
 
 // autotuner cache key of one pass of this handle's step
 std::string tune_key(const opfc_handle *h, const char *pass) {
-  static const char *models[] = {"plain", "tungsten", "filtered"};
+  static const char *models[] = {"plain", "tungsten", "filtered", "aluminum"};
   char b[160];
   std::snprintf(b, sizeof b, "step/%s/%s/%dx%dx%d/%s/f%s", h->prec == OPFC_FP64 ? "fp64" : "fp32",
                 models[h->desc.model], h->n0, h->n1, h->n2, pass,
@@ -383,8 +385,8 @@ int prepare_a(opfc_handle *h) {
     L.mode = COL_PLAIN;
     L.dir = +1;
     L.nsets = 1;
-    // psi part (TUNGSTEN) in A
-    if (model == OPFC_MODEL_TUNGSTEN) {
+    // psi part (two-field models) in A
+    if (two_field(model)) {
       L.in[0] = h->psi_hat;
       L.out[0] = h->work_a;
       L.in[1] = h->psi_hat;
@@ -393,7 +395,7 @@ int prepare_a(opfc_handle *h) {
       LAUNCH_TRY(h, col(h, L));
     }
     // chi * psi_hat -> scratch, then inverse z
-    void *dst = (model == OPFC_MODEL_TUNGSTEN) ? h->work_b : h->work_a;
+    void *dst = two_field(model) ? h->work_b : h->work_a;
     int rc = opfc_scale_by_table(h, h->psi_hat, h->tab_chi, dst);
     if (rc) return rc;
     LAUNCH_TRY(h, col_plain(h, 2, +1, dst, dst));
@@ -411,7 +413,7 @@ const char *const kStepKernelNames[kStepKernels] = {"y_inverse", "x_fused", "y_f
 int enqueue_step(opfc_handle *h, int only = -1) {
   const int model = h->desc.model;
   if (only < 0 || only == 0) {  // YI
-    if (model == OPFC_MODEL_TUNGSTEN)
+    if (two_field(model))
       LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_a, h->work_a, h->work_b, h->work_b));
     else
       LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_a, h->work_a));
@@ -429,6 +431,18 @@ int enqueue_step(opfc_handle *h, int only = -1) {
       X.c[0] = h->desc.p2 / 2.0;
       X.c[1] = h->desc.p3 / 3.0;
       X.c[2] = h->desc.p4 / 4.0;
+    } else if (model == OPFC_MODEL_ALUMINUM) {
+      // Aluminum.hpp:285-307 with the temperature offset T_var = 0 (G_grid = 0):
+      // N = p3_bar u^2 + p4_bar u^3 + q3 v^2 + q4_bar v^3 - stabP u,
+      // q3 = q31_bar T_const / T0 + q30_bar
+      X.model = MK_TUNGSTEN;
+      X.in1 = h->work_b;
+      const opfc_aluminum_params &p = h->desc.aluminum;
+      X.c[0] = p.p3_bar;
+      X.c[1] = p.p4_bar;
+      X.c[2] = p.q31_bar * p.T_const / p.T0 + p.q30_bar;
+      X.c[3] = p.q4_bar;
+      X.c[4] = p.stabP;
     } else {
       X.model = MK_TUNGSTEN;
       X.in1 = h->work_b;
@@ -453,7 +467,7 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     ColLaunch Z{};
     col_segments(h, 2, Z);
     Z.mode = COL_UPDATE;
-    Z.model = model == OPFC_MODEL_PLAIN ? MK_PLAIN : (model == OPFC_MODEL_TUNGSTEN ? MK_TUNGSTEN : MK_FILTERED);
+    Z.model = model == OPFC_MODEL_PLAIN ? MK_PLAIN : (two_field(model) ? MK_TUNGSTEN : MK_FILTERED);
     Z.inverse_after = 1;
     Z.nsets = 1;
     Z.in[0] = h->work_a;
@@ -467,7 +481,7 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.tab_chi = h->tab_chi;
     Z.axis = 2;
     // computed operators (variants 3, 4): PLAIN and FILTERED models
-    Z.computed = h->var_z >= 3 && model != OPFC_MODEL_TUNGSTEN;
+    Z.computed = h->var_z >= 3 && !two_field(model);
     Z.pingpong = h->var_z == 5;
     Z.rad_M = h->M;
     Z.rad_n1 = h->n1;
@@ -740,6 +754,7 @@ void opfc_desc_default(opfc_desc *d) {
   p.lambda = 0.22; p.stabP = 0.2; p.shift_u = 0.3341; p.shift_s = 0.1898;
   p.p2 = 1.0; p.p3 = -0.5; p.p4 = 0.333333333; p.q20 = -0.0037; p.q21 = 1.0;
   p.q30 = -12.4567; p.q31 = 20.0; p.q40 = 45.0;
+  d->aluminum.T0 = 1.0;  // Aluminum::params: everything 0 except T0 = 1
 }
 
 const char *opfc_status_string(int s) {
@@ -843,7 +858,7 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   std::unique_ptr<opfc_handle> h(new opfc_handle);
   h->desc = *d;
   if (d->precision != OPFC_FP32 && d->precision != OPFC_FP64) return OPFC_ERR_ARG;
-  if (d->model < OPFC_MODEL_PLAIN || d->model > OPFC_MODEL_FILTERED) return OPFC_ERR_ARG;
+  if (d->model < OPFC_MODEL_PLAIN || d->model > OPFC_MODEL_ALUMINUM) return OPFC_ERR_ARG;
   for (int a = 0; a < 3; ++a)
     if (d->n[a] < 1 || !(d->dx[a] > 0)) return OPFC_ERR_SIZE;
   if (d->n[0] < 2 || d->n[0] % 2 != 0) return OPFC_ERR_SIZE;
@@ -880,7 +895,7 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   };
   if ((rc = dev_alloc(hp, &hp->psi_hat, cb))) return cleanup(rc);
   if ((rc = dev_alloc(hp, &hp->work_a, cb))) return cleanup(rc);
-  if (d->model == OPFC_MODEL_TUNGSTEN && (rc = dev_alloc(hp, &hp->work_b, cb))) return cleanup(rc);
+  if (two_field(d->model) && (rc = dev_alloc(hp, &hp->work_b, cb))) return cleanup(rc);
   if ((rc = upload_twiddles(hp, hp->n0, &hp->tw_x))) return cleanup(rc);
   if ((rc = upload_twiddles(hp, hp->n1, &hp->tw_y))) return cleanup(rc);
   if ((rc = upload_twiddles(hp, hp->n2, &hp->tw_z))) return cleanup(rc);
@@ -920,12 +935,36 @@ int opfc_initialize(opfc_handle *h, double dt) {
   const double peak = P.Bx * std::exp(-P.T / P.T0);
   const double r = h->desc.r;
   const double fa = h->desc.filter_alpha;
+  const opfc_aluminum_params A = h->desc.aluminum;
+  if (model == OPFC_MODEL_ALUMINUM) {
+    if (A.G_grid != 0.0)
+      return fail(h, OPFC_ERR_ARG,
+                  "Aluminum: a moving temperature gradient (G_grid != 0) is not available on this path");
+    if (A.T0 == 0.0) return fail(h, OPFC_ERR_ARG, "Aluminum: T0 must be nonzero");
+  }
+  // Aluminum.hpp:186-242 (prepare_operators): chi = exp(kLap/(2 lambda^2)); the
+  // peak is the larger of the Gaussians around |k| = 1 and 2/sqrt(3);
+  // P_F = Bx exp(-tau_const) peak; opCk = stabP + p2_bar - P_F + q2_bar_L chi;
+  // opL = exp(kLap opCk dt); opN = kLap dt if opCk == 0 else (opL - 1)/opCk
+  auto aluminum_mode = [&](double kLap, double &oa, double &ob, double &oc) {
+    const double a2 = 2.0 * A.alpha * A.alpha, l2 = 2.0 * A.lambda * A.lambda;
+    const double fMF = std::exp(kLap / l2);
+    const double kw = std::sqrt(-kLap) - 1.0, kp = std::sqrt(-kLap) - 2.0 / std::sqrt(3.0);
+    const double g1 = std::exp(-(kw * kw) / a2), gp1 = std::exp(-(kp * kp) / a2);
+    const double PF = A.Bx * std::exp(-A.tau_const) * (g1 > gp1 ? g1 : gp1);
+    const double opCk = A.stabP + A.p2_bar - PF + A.q2_bar_L * fMF;
+    oa = std::exp(kLap * opCk * dt);
+    ob = (opCk == 0.0) ? kLap * dt : (oa - 1.0) / opCk;
+    oc = fMF;
+  };
   parallel_for((long)n2 * n1, [&](long row) {
     const int ky = (int)(row % n1), kz = (int)(row / n1);
     for (int kx = 0; kx < H; ++kx) {
       const double kx_ = kc(kx, n0, f0), ky_ = kc(ky, n1, f1), kz_ = kc(kz, n2, f2);
       const size_t o = split_index(h, kx, ky, kz);
-      if (model == OPFC_MODEL_TUNGSTEN) {
+      if (model == OPFC_MODEL_ALUMINUM) {
+        aluminum_mode(-((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_)), ta[o], tb[o], tc[o]);
+      } else if (model == OPFC_MODEL_TUNGSTEN) {
         // physics_for_mode (tungsten_spectral.hpp:83-104) + spectral_exp_coeffs
         // (spectral_exp_coefficients.hpp:68-82) + n_weight (tungsten_etd_workspace.hpp:111-130)
         const double kLap = -((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_));
@@ -985,7 +1024,9 @@ int opfc_initialize(opfc_handle *h, double dt) {
     std::vector<double> ops(2 * cnt), chi(need_chi ? cnt : 0);
     parallel_for((long)cnt, [&](long m) {
       const double k2 = f0 * f0 * (double)m;
-      if (model == OPFC_MODEL_TUNGSTEN) {
+      if (model == OPFC_MODEL_ALUMINUM) {
+        aluminum_mode(-k2, ops[2 * m], ops[2 * m + 1], chi[m]);
+      } else if (model == OPFC_MODEL_TUNGSTEN) {
         const double kLap = -k2;
         const double fMF = std::exp(kLap / lambda2);
         const double kv = std::sqrt(-kLap) - 1.0;
@@ -1036,7 +1077,7 @@ int opfc_initialize(opfc_handle *h, double dt) {
   if (const char *xv = std::getenv("OPFC_X_VARIANT")) h->var_x = std::atoi(xv);
   if (h->var_x < 0 || h->var_x >= kVarX) h->var_x = 0;
   if (h->var_z == 1 && !h->rad_ops) h->var_z = 0;
-  if (h->var_z >= 3 && model == OPFC_MODEL_TUNGSTEN) h->var_z = h->var_z == 4 ? 2 : 0;
+  if (h->var_z >= 3 && two_field(model)) h->var_z = h->var_z == 4 ? 2 : 0;
   if (h->var_z < 0 || h->var_z >= kVarZ) h->var_z = 0;
   if (h->var_y < 0 || h->var_y >= kVarY) h->var_y = 0;
   h->initialized = true;
@@ -1214,7 +1255,7 @@ int opfc_mass(opfc_handle *h, double *mean) {
 int opfc_free_energy(opfc_handle *h, double *energy) {
   if (!h || !energy) return OPFC_ERR_ARG;
   if (!h->have_state) return fail(h, OPFC_ERR_STATE, "no state");
-  if (h->desc.model == OPFC_MODEL_TUNGSTEN)
+  if (two_field(h->desc.model))
     return fail(h, OPFC_ERR_ARG, "free energy is defined for the plain and filtered models");
   CUDA_TRY(h, cudaSetDevice(h->device));
   // quadratic part by Parseval in k-space (FP64 accumulation of the resident state)
@@ -1262,7 +1303,7 @@ int opfc_autotune(opfc_handle *h, double *ms) {
       tune_key(h, "z"), kVarZ,
       [&](int v) {
         if (v == 1 && !h->rad_ops) return (int)OPFC_ERR_ARG;
-        if (v >= 3 && h->desc.model == OPFC_MODEL_TUNGSTEN) return (int)OPFC_ERR_ARG;
+        if (v >= 3 && two_field(h->desc.model)) return (int)OPFC_ERR_ARG;
         h->var_z = v;
         return enqueue_step(h, 3);
       },
@@ -1399,6 +1440,74 @@ int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, do
           psi[idx] = u;
         }
   }
+  return OPFC_OK;
+}
+
+// SeedGridFCC::apply (apps/aluminumNew/SeedGridFCC.hpp) with SeedFCC
+// (apps/aluminumNew/SeedFCC.hpp): one column of Ny x Nz seeds at x = X0 (Nx is
+// not used for placement), centres jittered by U(-0.2 r, 0.2 r) and Euler angles
+// U(0, 2 pi) from std::mt19937_64(rseed) through std::uniform_real_distribution
+// (drawn in the reference's order); inside |X - c| < r the value is
+// rho + sum_{4 <111>/sqrt(3) vectors q, rotated by yaw pitch roll} 2 amp cos(q . X)
+// with X the absolute coordinate; the first seed that contains a point wins.
+int opfc_ic_seed_grid_fcc(double *psi, const int n[3], const double dx[3], const double origin[3], int Nx, int Ny,
+                          int Nz, double X0, double radius, double amplitude, double rho, double rseed) {
+  if (!psi || !n || !dx || !origin || Nx < 1 || Ny < 1 || Nz < 1 || !(radius > 0)) return OPFC_ERR_ARG;
+  struct Seed {
+    double c[3], q[4][3];
+  };
+  const double Dy = dx[1] * n[1] / Ny, Dz = dx[2] * n[2] / Nz;
+  std::mt19937_64 re((std::mt19937_64::result_type)rseed);
+  std::uniform_real_distribution<double> rt(-0.2 * radius, 0.2 * radius);
+  std::uniform_real_distribution<double> rr(0.0, 8.0 * std::atan(1.0));
+  std::vector<Seed> seeds;
+  const double s = 1.0 / std::sqrt(3.0);
+  const double q0[4][3] = {{-s, s, s}, {s, -s, s}, {s, s, -s}, {s, s, s}};
+  for (int j = 0; j < Ny; ++j)
+    for (int k = 0; k < Nz; ++k) {
+      Seed sd;
+      sd.c[0] = X0 + rt(re);
+      sd.c[1] = Dy / 2.0 + Dy * j + rt(re);
+      sd.c[2] = Dz / 2.0 + Dz * k + rt(re);
+      double ang[3];
+      for (double &a : ang) a = rr(re);
+      const double ca = std::cos(ang[0]), sa = std::sin(ang[0]), cb = std::cos(ang[1]), sb = std::sin(ang[1]);
+      const double cc = std::cos(ang[2]), sc = std::sin(ang[2]);
+      const double Ra[3][3] = {{ca, -sa, 0}, {sa, ca, 0}, {0, 0, 1}};
+      const double Rb[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}};
+      const double Rc[3][3] = {{1, 0, 0}, {0, cc, -sc}, {0, sc, cc}};
+      double BC[3][3] = {}, R[3][3] = {};
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+          for (int c = 0; c < 3; ++c) BC[a][b] += Rb[a][c] * Rc[c][b];
+      for (int a = 0; a < 3; ++a)
+        for (int b = 0; b < 3; ++b)
+          for (int c = 0; c < 3; ++c) R[a][b] += Ra[a][c] * BC[c][b];
+      for (int v = 0; v < 4; ++v)
+        for (int a = 0; a < 3; ++a) {
+          double acc = 0;
+          for (int b = 0; b < 3; ++b) acc += R[a][b] * q0[v][b];
+          sd.q[v][a] = acc;
+        }
+      seeds.push_back(sd);
+    }
+  const double r2 = radius * radius;
+  parallel_for((long)n[2] * n[1], [&](long row) {
+    const int j = (int)(row % n[1]), k = (int)(row / n[1]);
+    const double y = origin[1] + j * dx[1], z = origin[2] + k * dx[2];
+    for (int i = 0; i < n[0]; ++i) {
+      const double x = origin[0] + i * dx[0];
+      for (const Seed &sd : seeds) {
+        const double ex = x - sd.c[0], ey = y - sd.c[1], ez = z - sd.c[2];
+        if (ex * ex + ey * ey + ez * ez < r2) {
+          double u = rho;
+          for (int v = 0; v < 4; ++v) u += 2.0 * amplitude * std::cos(sd.q[v][0] * x + sd.q[v][1] * y + sd.q[v][2] * z);
+          psi[(size_t)row * n[0] + i] = u;
+          break;
+        }
+      }
+    }
+  });
   return OPFC_OK;
 }
 
@@ -1618,7 +1727,7 @@ extern "C" {
 
 int opfc_set_r(opfc_handle *h, double r) {
   if (!h) return OPFC_ERR_ARG;
-  if (h->desc.model == OPFC_MODEL_TUNGSTEN) return fail(h, OPFC_ERR_ARG, "r is not a Tungsten parameter");
+  if (two_field(h->desc.model)) return fail(h, OPFC_ERR_ARG, "r is not a parameter of this model");
   h->desc.r = r;
   release_graph(h);
   h->ckpt_steps = 0;

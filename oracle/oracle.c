@@ -624,6 +624,110 @@ int orc_run_tungsten(const int n[3], const double dx[3],
   return 0;
 }
 
+/* ------------------------------------------------------------------------- */
+/* Aluminum PFC variant, apps/aluminumNew/Aluminum.hpp.                        */
+/* ------------------------------------------------------------------------- */
+
+/* Parameter block, names of Aluminum::params (Aluminum.hpp:29-82); the
+ * reference test leaves everything it does not set at 0 (T0 at 1). */
+typedef struct orc_aluminum_params {
+  double n0, n_sol, n_vap, T, T0, Bx, T_const, T_max, T_min, G_grid, V_grid, x_initial, m_xpos, alpha,
+      alpha_farTol;
+  int alpha_highOrd;
+  double tau_const, lambda, stabP, shift_u, shift_s, p2, p3, p4, p2_bar, p3_bar, p4_bar, q20, q21, q30, q31,
+      q40, q20_bar, q21_bar, q30_bar, q31_bar, q40_bar, q2_bar, q3_bar, q4_bar, q2_bar_L;
+} orc_aluminum_params;
+
+/* Operators per half-spectrum mode, Aluminum.hpp:186-242 (prepare_operators):
+ * chi = exp(kLap/(2 lambda^2)); the peak is the larger of the Gaussians around
+ * |k| = 1 and |k| = 2/sqrt(3); P_F = Bx exp(-tau_const) peak;
+ * opCk = stabP + p2_bar - P_F + q2_bar_L chi; opL = exp(kLap opCk dt);
+ * opN = kLap dt if opCk == 0 else (opL - 1)/opCk. */
+void orc_ops_aluminum(const int n[3], const double dx[3], const orc_aluminum_params *p, double dt,
+                      double *filterMF, double *opL, double *opN, double *P_F) {
+  const double fx = 2.0 * ORC_PI / (dx[0] * n[0]);
+  const double fy = 2.0 * ORC_PI / (dx[1] * n[1]);
+  const double fz = 2.0 * ORC_PI / (dx[2] * n[2]);
+  const int h = n[0] / 2 + 1;
+  const double alpha2 = 2.0 * p->alpha * p->alpha, lambda2 = 2.0 * p->lambda * p->lambda;
+  size_t idx = 0;
+  for (int k = 0; k < n[2]; ++k)
+    for (int j = 0; j < n[1]; ++j)
+      for (int i = 0; i < h; ++i, ++idx) {
+        const double ki = k_component(i, n[0], fx), kj = k_component(j, n[1], fy), kk = k_component(k, n[2], fz);
+        const double kLap = -(ki * ki + kj * kj + kk * kk);
+        const double fMF = exp(kLap / lambda2);
+        const double kw = sqrt(-kLap) - 1.0, kp = sqrt(-kLap) - 2.0 / sqrt(3.0);
+        const double g1 = exp(-(kw * kw) / alpha2), gp1 = exp(-(kp * kp) / alpha2);
+        const double peak = g1 > gp1 ? g1 : gp1;
+        const double PF = p->Bx * exp(-p->tau_const) * peak;
+        const double opCk = p->stabP + p->p2_bar - PF + p->q2_bar_L * fMF;
+        filterMF[idx] = fMF;
+        opL[idx] = exp(kLap * opCk * dt);
+        opN[idx] = (opCk == 0.0) ? kLap * dt : (opL[idx] - 1.0) / opCk;
+        if (P_F) P_F[idx] = PF;
+      }
+}
+
+/* Aluminum::step(t), Aluminum.hpp:247-326: psi_MF = F^-1[chi psi_F],
+ * P*psi = F^-1[P_F psi_F]; with the moving temperature
+ * T_var(x, t) = G_grid (dist - x_initial - V_grid t), dist = x + fullruns -
+ * (x > steppoint) l, l = N0 dx, fullruns = floor(m_xpos/l) l,
+ * steppoint = fmod(m_xpos, l):
+ * N = p3_bar u^2 + p4_bar u^3 + q2N v + q3 v^2 + q4_bar v^3 - kernel,
+ * q2N = q21_bar T_var/T0, q3 = q31_bar (T_const + T_var)/T0 + q30_bar,
+ * kernel = -(1 - exp(-T_var/T0)) P*psi; minus stabP u; psi_F = opL psi_F +
+ * opN F[N]; psi = F^-1[psi_F].  Step s uses t = t0 + s dt_t. */
+int orc_run_aluminum(const int n[3], const double dx[3], const double origin[3], const orc_aluminum_params *p,
+                     double dt, double t0, double dt_t, double *psi, int nsteps, double *norms) {
+  const size_t nr = (size_t)n[0] * n[1] * n[2];
+  const size_t nc = (size_t)(n[0] / 2 + 1) * n[1] * n[2];
+  double *fMF = malloc(sizeof(double) * nc), *oL = malloc(sizeof(double) * nc);
+  double *oN = malloc(sizeof(double) * nc), *PF = malloc(sizeof(double) * nc);
+  double *pF = malloc(sizeof(double) * 2 * nc), *wF = malloc(sizeof(double) * 2 * nc);
+  double *pMF = malloc(sizeof(double) * nr), *Pp = malloc(sizeof(double) * nr), *Nr = malloc(sizeof(double) * nr);
+  if (!fMF || !oL || !oN || !PF || !pF || !wF || !pMF || !Pp || !Nr) return -2;
+  orc_ops_aluminum(n, dx, p, dt, fMF, oL, oN, PF);
+  const double l = n[0] * dx[0];
+  const double fullruns = floor(p->m_xpos / l) * l, steppoint = fmod(p->m_xpos, l);
+  for (int s = 0; s < nsteps; ++s) {
+    const double t = t0 + s * dt_t;
+    orc_r2c(n[0], n[1], n[2], psi, pF);
+    for (size_t i = 0; i < nc; ++i) {
+      wF[2 * i] = fMF[i] * pF[2 * i];
+      wF[2 * i + 1] = fMF[i] * pF[2 * i + 1];
+    }
+    orc_c2r(n[0], n[1], n[2], wF, pMF);
+    for (size_t i = 0; i < nc; ++i) {
+      wF[2 * i] = PF[i] * pF[2 * i];
+      wF[2 * i + 1] = PF[i] * pF[2 * i + 1];
+    }
+    orc_c2r(n[0], n[1], n[2], wF, Pp);
+    for (size_t idx = 0; idx < nr; ++idx) {
+      const int i = (int)(idx % (size_t)n[0]);
+      const double x = origin[0] + i * dx[0];
+      const double dist = x + fullruns - (x > steppoint) * l;
+      const double Tv = p->G_grid * (dist - p->x_initial - p->V_grid * t);
+      const double q2N = p->q21_bar * Tv / p->T0;
+      const double q3 = p->q31_bar * (p->T_const + Tv) / p->T0 + p->q30_bar;
+      const double u = psi[idx], v = pMF[idx];
+      const double kern = -(1.0 - exp(-Tv / p->T0)) * Pp[idx];
+      Nr[idx] = p->p3_bar * u * u + p->p4_bar * u * u * u + q2N * v + q3 * v * v + p->q4_bar * v * v * v - kern;
+    }
+    if (p->stabP != 0.0)
+      for (size_t i = 0; i < nr; ++i) Nr[i] = Nr[i] - p->stabP * psi[i];
+    orc_r2c(n[0], n[1], n[2], Nr, wF);
+    for (size_t i = 0; i < nc; ++i) {
+      pF[2 * i] = oL[i] * pF[2 * i] + oN[i] * wF[2 * i];
+      pF[2 * i + 1] = oL[i] * pF[2 * i + 1] + oN[i] * wF[2 * i + 1];
+    }
+    orc_c2r(n[0], n[1], n[2], pF, psi);
+    if (norms) norms[s] = sumsq(psi, nr);
+  }
+  free(fMF); free(oL); free(oN); free(PF); free(pF); free(wF); free(pMF); free(Pp); free(Nr);
+  return 0;
+}
+
 /* Mean-field-filtered PFC with a polynomial of the filtered density:
  * psi_MF = F^-1[chi F[psi]], chi = exp(-k^2/(2 alpha^2));
  * N = p2 psi_MF^2/2 + p3 psi_MF^3/3 + p4 psi_MF^4/4;

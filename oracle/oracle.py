@@ -50,6 +50,11 @@ def lib():
         L.orc_run_tungsten.argtypes = [ip, dp, ctypes.c_void_p, ctypes.c_double, dp,
                                        ctypes.c_int, dp]
         L.orc_run_filtered.argtypes = [ip, dp] + [ctypes.c_double] * 6 + [dp, ctypes.c_int, dp]
+        cd = ctypes.c_double
+        L.orc_ops_aluminum.argtypes = [ip, dp, ctypes.c_void_p, cd, dp, dp, dp, dp]
+        L.orc_run_aluminum.argtypes = [ip, dp, dp, ctypes.c_void_p, cd, cd, cd, dp, ctypes.c_int, dp]
+        L.orc_ic_seed_grid_fcc.argtypes = [dp, ip, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, cd, cd, cd,
+                                           cd, cd]
         L.orc_sum.argtypes = [dp, ctypes.c_size_t]
         L.orc_sum.restype = ctypes.c_double
         L.orc_free_energy_plain.argtypes = [ip, dp, ctypes.c_double, dp]
@@ -221,6 +226,59 @@ def run_tungsten(psi, dx, p: TungstenParams, dt, nsteps, norms=False):
     rc = lib().orc_run_tungsten(_ivec(n), _dvec(dx), ctypes.byref(p), dt, _dp(psi), nsteps, _dp(nv))
     assert rc == 0
     return (psi, nv[:nsteps]) if norms else psi
+
+
+class AluminumParams(ctypes.Structure):
+    """Aluminum::params (apps/aluminumNew/Aluminum.hpp:29-82); fields not set
+    stay 0 (T0 = 1), as in the reference's default-initialised struct."""
+    _fields_ = [(k, ctypes.c_double) for k in
+                ["n0", "n_sol", "n_vap", "T", "T0", "Bx", "T_const", "T_max", "T_min", "G_grid", "V_grid",
+                 "x_initial", "m_xpos", "alpha", "alpha_farTol"]] + [("alpha_highOrd", ctypes.c_int)] + \
+        [(k, ctypes.c_double) for k in
+         ["tau_const", "lambda_", "stabP", "shift_u", "shift_s", "p2", "p3", "p4", "p2_bar", "p3_bar", "p4_bar",
+          "q20", "q21", "q30", "q31", "q40", "q20_bar", "q21_bar", "q30_bar", "q31_bar", "q40_bar", "q2_bar",
+          "q3_bar", "q4_bar", "q2_bar_L"]]
+
+    @classmethod
+    def test_case(cls):
+        """The values apps/aluminumNew/aluminumTest.cpp:52-80 sets (others 0, T0 from the test)."""
+        p = cls()
+        p.T0 = 1.0
+        for k, v in dict(n0=-0.0060, alpha=0.20, n_sol=-0.036, n_vap=-1.297, T_const=980, T_min=780,
+                         T_max=1280, T0=89285.0, Bx=0.817900686921996, G_grid=0, V_grid=0, x_initial=130,
+                         alpha_farTol=0.001, lambda_=0.22, stabP=0.0, shift_u=1.0, shift_s=0.0,
+                         p2_bar=0.8286531831, p3_bar=-0.04204863, p4_bar=0.007533, q20_bar=0.016531729105214,
+                         q21_bar=5.467, q30_bar=1.7152418049986, q31_bar=0.45, q40_bar=0.787482).items():
+            setattr(p, k, v)
+        p.alpha_highOrd = 0
+        return p
+
+
+def ops_aluminum(n, dx, p: AluminumParams, dt):
+    nc = (n[0] // 2 + 1) * n[1] * n[2]
+    out = [np.zeros(nc) for _ in range(4)]
+    lib().orc_ops_aluminum(_ivec(n), _dvec(dx), ctypes.byref(p), dt, *[_dp(o) for o in out])
+    return out  # filterMF, opL, opN, P_F
+
+
+def run_aluminum(psi, dx, origin, p: AluminumParams, dt, nsteps, t0=0.0, dt_t=0.0, norms=False):
+    """Aluminum steps; step s is called with time t0 + s dt_t."""
+    psi = np.ascontiguousarray(psi, dtype=np.float64).copy()
+    n = (psi.shape[2], psi.shape[1], psi.shape[0])
+    nv = np.zeros(max(nsteps, 1))
+    rc = lib().orc_run_aluminum(_ivec(n), _dvec(dx), _dvec(origin), ctypes.byref(p), dt, t0, dt_t, _dp(psi),
+                                nsteps, _dp(nv))
+    assert rc == 0
+    return (psi, nv[:nsteps]) if norms else psi
+
+
+def ic_seed_grid_fcc(psi, dx, origin, Nx, Ny, Nz, X0, radius, amplitude, rho, rseed):
+    """SeedGridFCC::apply on a pre-filled field (apps/aluminumNew/SeedGridFCC.hpp)."""
+    psi = np.ascontiguousarray(psi, dtype=np.float64).copy()
+    n = (psi.shape[2], psi.shape[1], psi.shape[0])
+    lib().orc_ic_seed_grid_fcc(_dp(psi), _ivec(n), _dvec(dx), _dvec(origin), int(Nx), int(Ny), int(Nz),
+                               float(X0), float(radius), float(amplitude), float(rho), float(rseed))
+    return psi
 
 
 def run_filtered(psi, dx, r, alpha, p2, p3, p4, dt, nsteps, norms=False):

@@ -2,11 +2,13 @@
 // reference's tests use pfc::fft::IFFT and the Tungsten model:
 //   - FFT known answers (tests/unit/kernel/fft/test_fft.cpp:28-70)
 //   - Tungsten golden L2^2 norms at 32^3 (apps/tungsten/tests/test_tungsten.cpp:177-356),
+//   - Aluminum golden norms at 32^3 (apps/aluminumNew/aluminumTest.cpp:48-110),
 //     initial condition applied to the host field exactly as that test does
 //   - plain PFC: mean density conserved, free energy finite
 // usage: test_adapters <tests/golden/tungsten_norms_32.json>; exit code 0 on success.
 #include <openpfc_b200/pfc_b200.hpp>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <fstream>
@@ -120,6 +122,49 @@ int main(int argc, char **argv) {
     for (int stp = 0; stp < 5; ++stp) pfcm.step(0.5 * stp);
     EXPECT(std::abs(pfcm.mean_density() - m0) <= 1e-15, "mean density %.17g vs %.17g", pfcm.mean_density(), m0);
     EXPECT(std::isfinite(pfcm.free_energy()), "free energy");
+  }
+  {  // Aluminum golden norms, written as apps/aluminumNew/aluminumTest.cpp:48-110 is
+    pfc::b200::AluminumB200<double> aluminum({32, 32, 32}, {1.0, 1.0, 1.0});
+    aluminum.set_n0(-0.0060);
+    aluminum.set_alpha(0.20);
+    aluminum.set_n_sol(-0.036);
+    aluminum.set_n_vap(-1.297);
+    aluminum.set_T_const(980);
+    aluminum.set_T_min(780);
+    aluminum.set_T_max(1280);
+    aluminum.set_T0(89285.0);
+    aluminum.set_Bx(0.817900686921996);
+    aluminum.set_G_grid(0);
+    aluminum.set_V_grid(0);
+    aluminum.set_x_initial(130);
+    aluminum.set_alpha_farTol(0.001);
+    aluminum.set_alpha_highOrd(0);
+    aluminum.set_lambda(0.22);
+    aluminum.set_stabP(0.0);
+    aluminum.set_shift_u(1.0);
+    aluminum.set_shift_s(0.0);
+    aluminum.set_p2_bar(0.8286531831);
+    aluminum.set_p3_bar(-0.04204863);
+    aluminum.set_p4_bar(0.007533);
+    aluminum.set_q20_bar(0.016531729105214);
+    aluminum.set_q21_bar(5.467);
+    aluminum.set_q30_bar(1.7152418049986);
+    aluminum.set_q31_bar(0.45);
+    aluminum.set_q40_bar(0.787482);
+    aluminum.initialize(1.0e-2);
+    std::vector<double> &psi = aluminum.get_real_field("psi");
+    std::fill(psi.begin(), psi.end(), -0.0060);
+    const int n[3] = {32, 32, 32};
+    const double dx1[3] = {1, 1, 1}, o[3] = {0, 0, 0};
+    opfc_ic_seed_grid_fcc(psi.data(), n, dx1, o, 1, 2, 2, 8.0, 4.0, 0.4, -0.036, 42);
+    const double expected[5] = {1297.08, 1250.21, 1209.28, 1173.19, 1141.09};
+    for (int i = 0; i < 5; ++i) {
+      std::vector<double> &p = aluminum.get_real_field("psi");
+      double norm2 = 0.0;
+      for (double x : p) norm2 += x * x;
+      EXPECT(std::abs(norm2 - expected[i]) <= 0.1, "aluminum norm %d: %.6f vs %.2f", i, norm2, expected[i]);
+      aluminum.step(1.0);
+    }
   }
   std::printf(failures ? "FAILED (%d)\n" : "OK\n", failures);
   return failures ? 1 : 0;

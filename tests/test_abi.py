@@ -85,3 +85,18 @@ def test_ic_generators_match_oracle(oracle):
     a = ob.ic_seed(np.full((16, 16, 16), -0.4), [d] * 3, origin, [0, 0, 0], 8.0, -0.047, 0.215936)
     b = oracle.ic_seed_inside(np.full((16, 16, 16), -0.4), [d] * 3, origin, 8.0, -0.047, 0.215936)
     np.testing.assert_allclose(a, b, rtol=0, atol=1e-15)
+
+
+def test_seed_grid_fcc_matches_oracle(oracle):
+    # the Aluminum test's initial condition (apps/aluminumNew/aluminumTest.cpp:83-96)
+    import numpy as np
+    base = np.full((32, 32, 32), -0.0060)
+    a = ob.ic_seed_grid_fcc(base, [1.0] * 3, [0.0] * 3, 1, 2, 2, 8.0, 4.0, 0.4, -0.036, 42)
+    b = oracle.ic_seed_grid_fcc(base, [1.0] * 3, [0.0] * 3, 1, 2, 2, 8.0, 4.0, 0.4, -0.036, 42)
+    np.testing.assert_array_equal(a, b)
+    assert abs(float((a ** 2).sum()) - 1297.08) <= 0.1
+    # anisotropic spacing, offset origin, several seeds
+    base = np.full((20, 24, 28), 0.1)
+    a = ob.ic_seed_grid_fcc(base, [0.7, 0.9, 1.1], [-2.0, 1.0, 0.5], 1, 3, 2, 6.0, 5.0, 0.3, -0.05, 7)
+    b = oracle.ic_seed_grid_fcc(base, [0.7, 0.9, 1.1], [-2.0, 1.0, 0.5], 1, 3, 2, 6.0, 5.0, 0.3, -0.05, 7)
+    np.testing.assert_array_equal(a, b)
