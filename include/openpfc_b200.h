@@ -165,7 +165,8 @@ const char *opfc_step_kernel_name(int k);
  * variants of each pass of the step (y: 0 pipelined | 1 direct | 2 pipelined
  * with half-width tiles, two CTAs per SM | 3 pipelined with ping-pong FFT
  * exchange buffers; x: 0 pipelined (warp-square kernel
- * where M = R^2 or 2 R^2) | 1 direct | 2 pipelined without it; z update:
+ * where M = R^2 or 2 R^2) | 1 direct | 2 pipelined without it | 3 warp-square
+ * with rows loaded straight into registers (PLAIN, FILTERED); z update:
  * 0 pipelined with streamed tables | 1 pipelined with radial tables (isotropic
  * grids) | 2 direct with streamed tables | 3 pipelined with operators computed
  * from k^2 | 4 direct with computed operators | 5 as 3 with ping-pong exchange
@@ -173,10 +174,10 @@ const char *opfc_step_kernel_name(int k);
  * 3 warm-up + 10 timed launches each), keeps the fastest and caches it per
  * device; opfc_initialize applies cached choices.  ms (OPFC_AUTOTUNE_SLOTS
  * doubles, may be NULL) receives the mean milliseconds per launch of
- * y0 y1 y2 y3 x0 x1 x2 z0 z1 z2 z3 z4 z5 (-1 if not applicable).  Call after
+ * y0 y1 y2 y3 x0 x1 x2 x3 z0 z1 z2 z3 z4 z5 (-1 if not applicable).  Call after
  * opfc_initialize; the passes run in place, so set the field afterwards.
  * opfc_variants reports the chosen (y, x, z) variants. */
-#define OPFC_AUTOTUNE_SLOTS 13
+#define OPFC_AUTOTUNE_SLOTS 14
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 

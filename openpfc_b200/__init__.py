@@ -229,6 +229,7 @@ class _ModelBase(_Handle):
         """Time every kernel variant of each pass, keep the fastest (cached per
         device); returns ms per launch by variant.  Set the field afterwards."""
         names = ["y.pipelined", "y.direct", "y.narrow", "y.pingpong", "x.pipelined", "x.direct", "x.no_square",
+                 "x.square_direct",
                  "z.tables", "z.radial", "z.direct", "z.computed", "z.direct_computed", "z.computed_pingpong"]
         ms = (ctypes.c_double * len(names))()
         _check(self._h, lib().opfc_autotune(self._h, ms))

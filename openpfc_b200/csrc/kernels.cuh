@@ -719,6 +719,24 @@ static int launch_x_sq(const XLaunch &L, cudaStream_t s) {
   return (int)cudaGetLastError();
 }
 
+template <typename Real, int R, int MODEL, int H>
+static int launch_x_sqd(const XLaunch &L, cudaStream_t s) {
+  using Cfg = XSqdCfg<Real, R, MODEL, H>;
+  if (L.rows % Cfg::ROWS != 0 || Cfg::SMEM > (size_t)kMaxDynSmem) return -1;
+  auto k = x_sqd_kernel<Real, R, MODEL, H>;
+  static int occ = 0;
+  if (!occ) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, Cfg::NT, Cfg::SMEM) != cudaSuccess || occ < 1)
+      occ = 1;
+  }
+  const int ngroups = L.rows / Cfg::ROWS;
+  int G = (L.num_sms > 0 ? L.num_sms : 148) * occ;
+  if (G > ngroups) G = ngroups;
+  k<<<G, Cfg::NT, Cfg::SMEM, s>>>(x_args<Real>(L));
+  return (int)cudaGetLastError();
+}
+
 template <typename Real, int M, int MODEL>
 static int launch_x_tma(const XLaunch &L, cudaStream_t s) {
   if constexpr (M < 16) {
@@ -799,6 +817,16 @@ template <typename Real, int M>
 static int launch_x_m(const XLaunch &L, cudaStream_t s) {
   if (L.mode == X_R2C) return launch_x_t<Real, M, X_R2C, 0>(L, s);
   if (L.mode == X_C2R) return launch_x_t<Real, M, X_C2R, 0>(L, s);
+  if (L.sq_direct) {  // warp-square transforms, rows loaded straight into registers
+    int rc = -1;
+    if constexpr (M == 64 || M == 256 || ((M == 128 || M == 512) && sizeof(Real) == 4)) {
+      constexpr int H = (M == 64 || M == 256) ? 1 : 2;
+      constexpr int R = (M == 64 || M == 128) ? 8 : 16;
+      if (L.model == MK_PLAIN) rc = launch_x_sqd<Real, R, MK_PLAIN, H>(L, s);
+      if (L.model == MK_FILTERED) rc = launch_x_sqd<Real, R, MK_FILTERED, H>(L, s);
+    }
+    if (rc >= 0) return rc;
+  }
   if (L.use_tma) {
     int rc = -1;
     if constexpr (M == 64 || M == 256) {

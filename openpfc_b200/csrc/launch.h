@@ -104,6 +104,7 @@ struct XLaunch {
   unsigned int *flag;  // bit 0: a non-finite value was produced; bit 1: a wait expired
   int use_tma;         // X_FUSED: persistent bulk-copy-fed kernel when the size allows
   int no_sq;           // X_FUSED: skip the warp-square kernel (x_sq.cuh) for x_tma.cuh
+  int sq_direct;       // X_FUSED: warp-square kernel with rows loaded straight into registers
   int num_sms;
 };
 

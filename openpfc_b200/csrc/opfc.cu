@@ -37,7 +37,7 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 4, kVarX = 3, kVarZ = 6;
+constexpr int kVarY = 4, kVarX = 4, kVarZ = 6;
 // models with two real fields per step (psi and psi_MF): Tungsten, Aluminum
 inline bool two_field(int model) { return model == OPFC_MODEL_TUNGSTEN || model == OPFC_MODEL_ALUMINUM; }  // kernel variants per pass (opfc_autotune)
 
@@ -132,7 +132,8 @@ struct opfc_handle {
   // var_y: 0 pipelined, 1 direct, 2 pipelined narrow tiles (two CTAs per SM),
   //        3 pipelined with ping-pong exchange buffers;
   // var_x: 0 pipelined (warp-square kernel where it applies), 1 direct,
-  //        2 pipelined without the warp-square kernel;
+  //        2 pipelined without the warp-square kernel, 3 warp-square kernel
+  //        with rows loaded straight into registers (PLAIN, FILTERED);
   // var_z: 0 pipelined with streamed tables, 1 pipelined with radial tables,
   //        2 direct with streamed tables, 3 pipelined with computed operators,
   //        4 direct with computed operators, 5 as 3 with ping-pong exchange
@@ -357,6 +358,7 @@ XLaunch x_base(opfc_handle *h) {
   L.flag = h->flag;
   L.use_tma = h->use_tma && h->var_x != 1;
   L.no_sq = h->var_x == 2;
+  L.sq_direct = h->var_x == 3;
   L.num_sms = h->num_sms;
   return L;
 }

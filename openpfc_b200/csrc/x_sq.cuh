@@ -259,4 +259,118 @@ __global__ void __launch_bounds__(XSqCfg<Real, R, MODEL, H>::W *R) x_sq_kernel(c
   }
 }
 
+// ---------------------------------------------------------------------------
+// Direct-load form (no staging ring): each lane loads its E values of the row
+// straight from HBM (k = j + R m: 128-byte coalesced segments), parks them in
+// the row's warp-private buffer in natural order, and the C2R pre-processing
+// reads X[k] and X[M-k] from there; the rest is the kernel above.  Without the
+// staged tiles a CTA needs only the exchange buffers, so more warps fit per SM
+// (registers, not shared memory, bound the occupancy) and no CTA barrier runs
+// inside the loop.  One field per row (PLAIN, FILTERED).
+// ---------------------------------------------------------------------------
+template <typename Real, int R, int MODEL, int H> struct XSqdCfg {
+  using C = typename CxP<Real>::T;
+  static constexpr int M = H * R * R;
+  static constexpr int E = H * R;
+  static constexpr int NT = 256;
+  static constexpr int ROWS = NT / R;  // rows per CTA pass
+  static constexpr int EXL0 = R * (R + 1);
+  static constexpr int EXL = EXL0 > M + 1 ? EXL0 : M + 1;
+  static constexpr size_t TW = align128(size_t(M) * sizeof(C));
+  static constexpr size_t TWS = align128(size_t(R) * R * sizeof(C));
+  static constexpr size_t SMEM = TW + TWS + size_t(ROWS) * EXL * sizeof(C);
+};
+
+template <typename Real, int R, int MODEL, int H>
+__global__ void __launch_bounds__(256, H == 1 ? 4 : 2) x_sqd_kernel(const XArgs<Real> a) {
+  using Cfg = XSqdCfg<Real, R, MODEL, H>;
+  using C = typename CxP<Real>::T;
+  constexpr int M = Cfg::M;
+  constexpr int E = Cfg::E;
+  constexpr int NT = Cfg::NT;
+  constexpr int ROWS = Cfg::ROWS;
+  constexpr int N0 = 2 * M;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *tws = reinterpret_cast<C *>(smraw + Cfg::TW);
+  C *exall = reinterpret_cast<C *>(smraw + Cfg::TW + Cfg::TWS);
+
+  const int tid = threadIdx.x;
+  const int j = tid % R;
+  const int c = tid / R;
+  const int lane = tid & 31;
+  const int partner = (lane & ~(R - 1)) | ((R - j) & (R - 1));
+  const C *gtw = reinterpret_cast<const C *>(a.tw);
+  for (int i = tid; i < M; i += NT) tw[i] = gtw[i];
+  for (int i = tid; i < (R - 1) * R; i += NT) {
+    const int r = i / R + 1, k = i % R;
+    tws[i] = gtw[((N0 / (R * R)) * k * r) % N0];
+  }
+  __syncthreads();
+
+  C *ex = exall + c * Cfg::EXL;
+  const C *in = reinterpret_cast<const C *>(a.in0);
+  C *out = reinterpret_cast<C *>(a.out);
+  const Real sc = (Real)a.scale, mn = (Real)a.mean;
+  bool bad = false;
+  for (long long row0 = (long long)blockIdx.x * ROWS; row0 < a.rows; row0 += (long long)gridDim.x * ROWS) {
+    const long long row = row0 + c;  // rows is a multiple of ROWS (launcher)
+    C v[E];
+#pragma unroll
+    for (int m = 0; m < E; ++m) v[m] = in[row * M + j + R * m];
+    const C nyq = in[a.nyq_off + row];
+    // natural order into the row buffer: ex[k] = X[k], ex[M] = X[M]
+#pragma unroll
+    for (int m = 0; m < E; ++m) ex[j + R * m] = v[m];
+    if (j == 0) ex[M] = nyq;
+    __syncwarp();
+    // C2R pre-processing (x_pre_rows): Z'[k] from X[k] and X[M-k]
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int k = j + R * m;
+      C X = v[m];
+      C Y = ex[M - k];
+      if (k == 0) {
+        X.y = 0;
+        Y.y = 0;
+      }
+      const C s2 = mk<C>(X.x + Y.x, X.y - Y.y);
+      const C d = mk<C>(X.x - Y.x, X.y + Y.y);
+      const C e = twmul<+1>(d, tw[k]);
+      v[m] = mk<C>(s2.x - e.y, s2.y + e.x);
+    }
+    __syncwarp();  // row buffer free: it becomes the FFT exchange space
+    fft_sq_dif<C, R, H, +1>(v, ex, j, tws, tw);
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const Real x = v[m].x * sc + mn, y = v[m].y * sc + mn;
+      Real nx, ny;
+      if constexpr (MODEL == MK_FILTERED) {
+        nx = x * x * (a.c0 + a.c1 * x + a.c2 * x * x);
+        ny = y * y * (a.c0 + a.c1 * y + a.c2 * y * y);
+      } else {
+        nx = x * x * x;
+        ny = y * y * y;
+      }
+      bad |= !(isfinite(nx) && isfinite(ny));
+      v[m] = mk<C>(nx, ny);
+    }
+    fft_sq_dit<C, R, H, -1>(v, ex, j, tws, tw);
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+      const int k = j + R * m;
+      C Y = shfl_c(v[E - 1 - m], partner);
+      if (j == 0) Y = v[(E - m) % E];
+      const C Z = v[m];
+      const C sm = mk<C>(Z.x + Y.x, Z.y - Y.y);
+      const C d = mk<C>(Z.x - Y.x, Z.y + Y.y);
+      const C e = twmul<-1>(d, tw[k]);
+      out[row * M + k] = mk<C>(Real(0.5) * (sm.x + e.y), Real(0.5) * (sm.y - e.x));
+    }
+    if (j == 0) out[a.nyq_off + row] = mk<C>(v[0].x - v[0].y, Real(0));
+    __syncwarp();  // exchange space reused by the next row
+  }
+  if (bad && a.flag) atomicOr(a.flag, 1u);
+}
+
 }  // namespace opfc

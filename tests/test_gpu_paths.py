@@ -25,7 +25,8 @@ def path(request, monkeypatch):
     without the warp-square kernel (OPFC_X_VARIANT=2);
     direct_computed: direct z update computing its operators (OPFC_Z_VARIANT=4);
     pingpong: ping-pong FFT exchange buffers in the y pass and the computed
-    z update (OPFC_Y_VARIANT=3, OPFC_Z_VARIANT=5).
+    z update (OPFC_Y_VARIANT=3, OPFC_Z_VARIANT=5), and the x pass's warp-square
+    kernel with rows loaded straight into registers (OPFC_X_VARIANT=3).
     The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
@@ -45,6 +46,7 @@ def path(request, monkeypatch):
     elif request.param == "pingpong":
         monkeypatch.setenv("OPFC_Y_VARIANT", "3")
         monkeypatch.setenv("OPFC_Z_VARIANT", "5")
+        monkeypatch.setenv("OPFC_X_VARIANT", "3")
     return request.param
 
 
