@@ -164,7 +164,8 @@ const char *opfc_step_kernel_name(int k);
  * variables OPENPFC_GPU_AUTOTUNE_{DISABLE,MODE,CACHE_DIR}): times the kernel
  * variants of each pass of the step (y: 0 pipelined | 1 direct | 2 pipelined
  * with half-width tiles, two CTAs per SM | 3 pipelined with ping-pong FFT
- * exchange buffers; x: 0 pipelined (warp-square kernel
+ * exchange buffers | 4 direct with 32 values per thread (N = 512, 1024); x: 0
+ * pipelined (warp-square kernel
  * where M = R^2 or 2 R^2) | 1 direct | 2 pipelined without it | 3 warp-square
  * with rows loaded straight into registers (PLAIN, FILTERED); z update:
  * 0 pipelined with streamed tables | 1 pipelined with radial tables (isotropic
@@ -174,10 +175,10 @@ const char *opfc_step_kernel_name(int k);
  * 3 warm-up + 10 timed launches each), keeps the fastest and caches it per
  * device; opfc_initialize applies cached choices.  ms (OPFC_AUTOTUNE_SLOTS
  * doubles, may be NULL) receives the mean milliseconds per launch of
- * y0 y1 y2 y3 x0 x1 x2 x3 z0 z1 z2 z3 z4 z5 (-1 if not applicable).  Call after
+ * y0 .. y4 x0 .. x3 z0 .. z5 (-1 if not applicable).  Call after
  * opfc_initialize; the passes run in place, so set the field afterwards.
  * opfc_variants reports the chosen (y, x, z) variants. */
-#define OPFC_AUTOTUNE_SLOTS 14
+#define OPFC_AUTOTUNE_SLOTS 15
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 

@@ -228,7 +228,8 @@ class _ModelBase(_Handle):
     def autotune(self) -> dict:
         """Time every kernel variant of each pass, keep the fastest (cached per
         device); returns ms per launch by variant.  Set the field afterwards."""
-        names = ["y.pipelined", "y.direct", "y.narrow", "y.pingpong", "x.pipelined", "x.direct", "x.no_square",
+        names = ["y.pipelined", "y.direct", "y.narrow", "y.pingpong", "y.direct_e32", "x.pipelined", "x.direct",
+                 "x.no_square",
                  "x.square_direct",
                  "z.tables", "z.radial", "z.direct", "z.computed", "z.direct_computed", "z.computed_pingpong"]
         ms = (ctypes.c_double * len(names))()

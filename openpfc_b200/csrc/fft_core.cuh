@@ -160,6 +160,61 @@ template <int DIR, typename C> struct Dft<16, DIR, C> {
   }
 };
 
+// 32 = 2 x 16 (decimation in time): E, O = DFT16 of the even / odd samples,
+// X[k] = E[k] + W32^k O[k], X[k + 16] = E[k] - W32^k O[k], W32 = exp(DIR 2 pi i / 32).
+template <int DIR, typename C> struct Dft<32, DIR, C> {
+  static __device__ __forceinline__ void run(C (&v)[32]) {
+    using S = decltype(C::x);
+    // cos(pi k / 16) and sin(pi k / 16), k = 0..15
+    constexpr double cs[16] = {1.0,
+                               0.980785280403230449126182236134239037,
+                               0.923879532511286756128183189396788287,
+                               0.831469612302545237078788377617905757,
+                               0.707106781186547524400844362104849039,
+                               0.555570233019602224742830813948532874,
+                               0.382683432365089771728459984030398867,
+                               0.195090322016128267848284868477022241,
+                               0.0,
+                               -0.195090322016128267848284868477022241,
+                               -0.382683432365089771728459984030398867,
+                               -0.555570233019602224742830813948532874,
+                               -0.707106781186547524400844362104849039,
+                               -0.831469612302545237078788377617905757,
+                               -0.923879532511286756128183189396788287,
+                               -0.980785280403230449126182236134239037};
+    constexpr double sn[16] = {0.0,
+                               0.195090322016128267848284868477022241,
+                               0.382683432365089771728459984030398867,
+                               0.555570233019602224742830813948532874,
+                               0.707106781186547524400844362104849039,
+                               0.831469612302545237078788377617905757,
+                               0.923879532511286756128183189396788287,
+                               0.980785280403230449126182236134239037,
+                               1.0,
+                               0.980785280403230449126182236134239037,
+                               0.923879532511286756128183189396788287,
+                               0.831469612302545237078788377617905757,
+                               0.707106781186547524400844362104849039,
+                               0.555570233019602224742830813948532874,
+                               0.382683432365089771728459984030398867,
+                               0.195090322016128267848284868477022241};
+    C e[16], o[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      e[i] = v[2 * i];
+      o[i] = v[2 * i + 1];
+    }
+    Dft<16, DIR, C>::run(e);
+    Dft<16, DIR, C>::run(o);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const C t = k == 0 ? o[0] : Dft<16, DIR, C>::w(o[k], S(cs[k]), S(sn[k]));
+      v[k] = cadd(e[k], t);
+      v[k + 16] = csub(e[k], t);
+    }
+  }
+};
+
 template <int DIR, typename C> struct Dft<3, DIR, C> {
   static __device__ __forceinline__ void run(C (&v)[3]) {
     using S = decltype(C::x);
@@ -281,6 +336,9 @@ template <> struct PlanE<16, 4> { using R = Radices<4, 4>; };
 template <> struct PlanE<24, 6> { using R = Radices<2, 2, 2, 3>; };
 template <> struct PlanE<40, 10> { using R = Radices<2, 2, 2, 5>; };
 template <> struct PlanE<64, 16> { using R = Radices<8, 8>; };
+// one shared-memory exchange per transform (32 values per thread)
+template <> struct PlanE<512, 32> { using R = Radices<16, 32>; };
+template <> struct PlanE<1024, 32> { using R = Radices<32, 32>; };
 
 template <typename C, int N, int E, int DIR, int TWS, int... Rs>
 __device__ __forceinline__ void fft_run(Radices<Rs...>, C (&v)[E], C *sm, int ld, int c, int j,

@@ -79,11 +79,13 @@ namespace opfc {
 // ---------------------------------------------------------------------------
 // column pass: batched FFT along a strided axis (y or z), optional ETD update
 // ---------------------------------------------------------------------------
-template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS>
-__global__ void __launch_bounds__(Width<Real>::W *(N / Plan<N>::E)) col_kernel(const ColArgs<Real> a) {
+// EE values per thread (plan PlanE<N, EE>; EE = 32 gives one exchange per
+// transform at N = 512, 1024).
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS, int EE = Plan<N>::E>
+__global__ void __launch_bounds__(Width<Real>::W *(N / EE)) col_kernel(const ColArgs<Real> a) {
   using C = typename Cx<Real>::T;
   constexpr int W = Width<Real>::W;
-  constexpr int E = Plan<N>::E;
+  constexpr int E = EE;
   constexpr int T = N / E;
   constexpr int NT = W * T;
   constexpr int ld = W + 1;
@@ -116,14 +118,14 @@ __global__ void __launch_bounds__(Width<Real>::W *(N / Plan<N>::E)) col_kernel(c
   for (int m = 0; m < E; ++m) v[m] = ok ? in[base + (long long)(j + T * m) * fs] : czero<C>();
 
   if constexpr (MODE == COL_PLAIN) {
-    fft_line<C, N, DIR, N>(v, sm, ld, c, j, tw);
+    fft_line_e<C, N, DIR, N, E>(v, sm, ld, c, j, tw);
     if (ok) {
 #pragma unroll
       for (int m = 0; m < E; ++m) out[base + (long long)(j + T * m) * fs] = v[m];
     }
   } else {
     // forward z transform completes N_hat; ETD update of the resident state
-    fft_line<C, N, -1, N>(v, sm, ld, c, j, tw);
+    fft_line_e<C, N, -1, N, E>(v, sm, ld, c, j, tw);
     C *ph = reinterpret_cast<C *>(a.psi_hat);
     C w[(MODEL == MK_PLAIN) ? 1 : E];
 #pragma unroll
@@ -151,20 +153,20 @@ __global__ void __launch_bounds__(Width<Real>::W *(N / Plan<N>::E)) col_kernel(c
     }
     if constexpr (INV) {
       if constexpr (MODEL == MK_FILTERED) {
-        fft_line<C, N, +1, N>(w, sm, ld, c, j, tw);
+        fft_line_e<C, N, +1, N, E>(w, sm, ld, c, j, tw);
         if (ok) {
 #pragma unroll
           for (int m = 0; m < E; ++m) out[base + (long long)(j + T * m) * fs] = w[m];
         }
       } else {
-        fft_line<C, N, +1, N>(v, sm, ld, c, j, tw);
+        fft_line_e<C, N, +1, N, E>(v, sm, ld, c, j, tw);
         if (ok) {
 #pragma unroll
           for (int m = 0; m < E; ++m) out[base + (long long)(j + T * m) * fs] = v[m];
         }
         if constexpr (MODEL == MK_TUNGSTEN) {
           C *out2 = reinterpret_cast<C *>(a.out[1]);
-          fft_line<C, N, +1, N>(w, sm, ld, c, j, tw);
+          fft_line_e<C, N, +1, N, E>(w, sm, ld, c, j, tw);
           if (ok) {
 #pragma unroll
             for (int m = 0; m < E; ++m) out2[base + (long long)(j + T * m) * fs] = w[m];
@@ -580,13 +582,13 @@ template <typename Real> static ColArgs<Real> col_args(const ColLaunch &L) {
   return a;
 }
 
-template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS>
+template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV, int OPS, int EE = Plan<N>::E>
 static int launch_col_direct(const ColLaunch &L, cudaStream_t s) {
   using C = typename Cx<Real>::T;
   constexpr int W = Width<Real>::W;
-  constexpr int NT = W * (N / Plan<N>::E);
+  constexpr int NT = W * (N / EE);
   const size_t smem = sizeof(C) * ((size_t)N + (size_t)N * (W + 1));
-  auto k = col_kernel<Real, N, MODE, DIR, MODEL, INV, OPS>;
+  auto k = col_kernel<Real, N, MODE, DIR, MODEL, INV, OPS, EE>;
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -652,9 +654,14 @@ static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
                         : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false>(L, s);
     if (rc >= 0) return rc;
   }
+  // plain transforms with 32 values per thread: one shared-memory exchange per
+  // transform (N = 512, 1024)
+  constexpr bool E32 = (N == 512 || N == 1024);
   if constexpr (MODE == COL_UPDATE && MODEL != MK_TUNGSTEN) {
     if (L.computed) return launch_col_direct<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED>(L, s);
   }
+  if constexpr (MODE == COL_PLAIN && E32)
+    if (L.e32) return launch_col_direct<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, 32>(L, s);
   return launch_col_direct<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES>(L, s);
 }
 

@@ -68,6 +68,9 @@ struct ColLaunch {
   // ping-pong FFT exchange buffers (one CTA barrier per exchange; one ring
   // stage fewer): COL_PLAIN and the computed-operator update
   int pingpong;
+  // COL_PLAIN direct-load kernel with 32 values per thread (N = 512, 1024:
+  // one exchange per transform)
+  int e32;
   int axis;            // 1 = y, 2 = z
   unsigned int *flag;  // bit 1: a bounded wait expired
   int num_sms;

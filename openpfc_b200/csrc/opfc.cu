@@ -37,7 +37,7 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 4, kVarX = 4, kVarZ = 6;
+constexpr int kVarY = 5, kVarX = 4, kVarZ = 6;
 // models with two real fields per step (psi and psi_MF): Tungsten, Aluminum
 inline bool two_field(int model) { return model == OPFC_MODEL_TUNGSTEN || model == OPFC_MODEL_ALUMINUM; }  // kernel variants per pass (opfc_autotune)
 
@@ -130,7 +130,8 @@ struct opfc_handle {
   bool use_tma = true;  // TMA-fed column passes (OPFC_NO_TMA=1 disables)
   // kernel variants per pass, chosen by the autotuner (see opfc_autotune):
   // var_y: 0 pipelined, 1 direct, 2 pipelined narrow tiles (two CTAs per SM),
-  //        3 pipelined with ping-pong exchange buffers;
+  //        3 pipelined with ping-pong exchange buffers, 4 direct with 32
+  //        values per thread (one exchange per transform at N = 512, 1024);
   // var_x: 0 pipelined (warp-square kernel where it applies), 1 direct,
   //        2 pipelined without the warp-square kernel, 3 warp-square kernel
   //        with rows loaded straight into registers (PLAIN, FILTERED);
@@ -305,8 +306,9 @@ int col_plain(opfc_handle *h, int axis, int dir, const void *in0, void *out0,
   L.axis = axis;
   L.narrow = h->var_y == 2;
   L.pingpong = h->var_y == 3;
+  L.e32 = h->var_y == 4;
   const int W = tma_col_width(L.N, 2 * (int)h->rsz, COL_PLAIN, L.narrow);
-  if (h->use_tma && h->var_y != 1 && L.N > 1 && h->M % W == 0) {
+  if (h->use_tma && h->var_y != 1 && h->var_y != 4 && L.N > 1 && h->M % W == 0) {
     L.tmap[0] = tmap_for(h, in0, axis, W, false);
     L.tmap[1] = in1 ? tmap_for(h, in1, axis, W, false) : nullptr;
     if (in1 && !L.tmap[1]) L.tmap[0] = nullptr;

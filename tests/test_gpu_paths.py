@@ -14,7 +14,7 @@ pytestmark = pytest.mark.gpu
 PI4 = [math.pi / 4] * 3
 
 
-@pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "pingpong"])
+@pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "pingpong", "e32"])
 def path(request, monkeypatch):
     """tma: pipelined kernels streaming the per-mode tables (default);
     tma_radial: the z update reading radial operator tables (OPFC_Z_VARIANT=1,
@@ -26,7 +26,9 @@ def path(request, monkeypatch):
     direct_computed: direct z update computing its operators (OPFC_Z_VARIANT=4);
     pingpong: ping-pong FFT exchange buffers in the y pass and the computed
     z update (OPFC_Y_VARIANT=3, OPFC_Z_VARIANT=5), and the x pass's warp-square
-    kernel with rows loaded straight into registers (OPFC_X_VARIANT=3).
+    kernel with rows loaded straight into registers (OPFC_X_VARIANT=3);
+    e32: direct-load y pass with 32 values per thread (OPFC_Y_VARIANT=4;
+    other lengths keep their plan).
     The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
@@ -47,6 +49,8 @@ def path(request, monkeypatch):
         monkeypatch.setenv("OPFC_Y_VARIANT", "3")
         monkeypatch.setenv("OPFC_Z_VARIANT", "5")
         monkeypatch.setenv("OPFC_X_VARIANT", "3")
+    elif request.param == "e32":
+        monkeypatch.setenv("OPFC_Y_VARIANT", "4")
     return request.param
 
 
