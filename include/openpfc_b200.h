@@ -64,8 +64,10 @@ typedef struct opfc_tungsten_params {
 
 /* Aluminum PFC parameters: the fields of Aluminum::params
  * (apps/aluminumNew/Aluminum.hpp:29-82), same names; the reference leaves
- * unset fields at 0 (opfc_desc_default: all 0, T0 = 1).  The GPU path takes
- * G_grid = 0 (no moving temperature gradient; G_grid != 0 is refused). */
+ * unset fields at 0 (opfc_desc_default: all 0, T0 = 1).  With G_grid != 0 the
+ * step carries the moving temperature T_var(x, t) and a third field
+ * P*psi = F^-1[P_F psi_hat] (direct-load kernels); its time comes from
+ * opfc_set_time. */
 typedef struct opfc_aluminum_params {
   double n0, n_sol, n_vap, T, T0, Bx, T_const, T_max, T_min, G_grid, V_grid, x_initial, m_xpos, alpha,
       alpha_farTol;
@@ -214,6 +216,11 @@ size_t opfc_ensemble_cells(const opfc_ensemble *e);
 void *opfc_ensemble_stream(const opfc_ensemble *e);
 
 int opfc_set_r(opfc_handle *h, double r);
+/* Time of the next step for models whose step depends on it (Aluminum with a
+ * moving temperature gradient: the t of Aluminum::step(t)); each step then
+ * advances it by dt_per_step on the device (opfc_initialize sets the time to 0
+ * and the increment to dt).  Other models ignore it. */
+int opfc_set_time(opfc_handle *h, double t, double dt_per_step);
 int opfc_forward_checkpointed(opfc_handle *h, int n_steps, int K);
 int opfc_adjoint(opfc_handle *h, const void *grad_psi_T, int dtype, int where, void *grad_psi0,
                  double *grad_r, double *grad_n0);

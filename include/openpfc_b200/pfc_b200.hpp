@@ -287,8 +287,9 @@ template <typename T = double> class TungstenB200 : public detail::ModelBase<T> 
 
 /// Aluminum PFC variant (apps/aluminumNew/Aluminum.hpp): fields "psi",
 /// "default" and "psiMF"; the same setters as Aluminum (set_n0 ... set_q2_bar_L)
-/// on a parameter block that starts at 0 (T0 = 1) like Aluminum::params.  The
-/// moving temperature gradient (G_grid != 0) is refused by initialize().
+/// on a parameter block that starts at 0 (T0 = 1) like Aluminum::params.
+/// step(t) uses t for the moving temperature T_var(x, t) (G_grid != 0), as
+/// Aluminum::step(t) does.
 template <typename T = double> class AluminumB200 : public detail::ModelBase<T> {
  public:
   AluminumB200(std::array<int, 3> n, std::array<double, 3> dx, std::array<double, 3> origin = {}, int device = 0)
@@ -301,6 +302,10 @@ template <typename T = double> class AluminumB200 : public detail::ModelBase<T> 
     this->fields_["psiMF"];
   }
   opfc_aluminum_params params;
+  void step(double t) override {
+    check(opfc_set_time(this->h_, t, 0.0), "step", opfc_last_error(this->h_));
+    detail::ModelBase<T>::step(t);
+  }
 #define OPFC_ALU(name, type) \
   void set_##name(type v) { params.name = v; }
   OPFC_ALU(n0, double)

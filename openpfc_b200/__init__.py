@@ -324,8 +324,12 @@ class TungstenB200(_ModelBase):
 class AluminumB200(_ModelBase):
     """Aluminum PFC variant (apps/aluminumNew/Aluminum.hpp): Tungsten-form step
     with the two-Gaussian correlation peak P_F; ``params`` is an AluminumParams
-    (fields the caller leaves unset stay 0, T0 = 1, as in the reference).  The
-    moving temperature gradient (G_grid != 0) is refused by initialize()."""
+    (fields the caller leaves unset stay 0, T0 = 1, as in the reference).  With
+    G_grid != 0 the moving temperature T_var(x, t) acts: set_time(t, dt_t) gives
+    the time of the next step (then advanced by dt_t per step)."""
+
+    def set_time(self, t: float, dt_per_step: float):
+        _check(self._h, lib().opfc_set_time(self._h, float(t), float(dt_per_step)))
 
     def __init__(self, n, dx, params: AluminumParams | None = None, precision: int = FP64,
                  device: int = 0, origin=None, stream=None):

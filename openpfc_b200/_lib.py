@@ -124,6 +124,7 @@ def lib():
     L.opfc_write_binary_hat.argtypes = [H, cp, ci]
     L.opfc_read_binary.argtypes = [H, cp]
     L.opfc_write_vti.argtypes = [H, cp, ci, cp]
+    L.opfc_set_time.argtypes = [H, cd, cd]
     L.opfc_write_raw.argtypes = [cp, ip, ip, ip, dp, ci]
     L.opfc_read_raw.argtypes = [cp, ip, ip, ip, dp, ci]
     L.opfc_write_vti_raw.argtypes = [cp, ip, ip, ip, dp, dp, cp, dp]

@@ -30,6 +30,8 @@ template <typename Real> struct ColArgs {
   const void *tw;
   void *psi_hat;
   const Real *tab_a, *tab_b, *tab_chi;
+  const Real *tab_p;  // MK_ALUMINUM_G: P_F
+  void *out_p;        // MK_ALUMINUM_G: F_z^-1[P_F psi_hat]
   // radial operators (isotropic grids): rad_ops[m] = (opL, opN), rad_chi[m],
   // m = kx^2 + ky^2 + kz^2 in folded integer indices
   const void *rad_ops;
@@ -128,10 +130,12 @@ __global__ void __launch_bounds__(Width<Real>::W *(N / EE)) col_kernel(const Col
     fft_line_e<C, N, -1, N, E>(v, sm, ld, c, j, tw);
     C *ph = reinterpret_cast<C *>(a.psi_hat);
     C w[(MODEL == MK_PLAIN) ? 1 : E];
+    C pw[(MODEL == MK_ALUMINUM_G) ? E : 1];
 #pragma unroll
     for (int m = 0; m < E; ++m) {
       const long long idx = base + (long long)(j + T * m) * fs;
       C np = czero<C>();
+      if constexpr (MODEL == MK_ALUMINUM_G) pw[m] = czero<C>();
       if (ok) {
         const C p = ph[idx];
         Real la, lb, ch = Real(1);
@@ -146,6 +150,7 @@ __global__ void __launch_bounds__(Width<Real>::W *(N / EE)) col_kernel(const Col
         np = mk<C>(la * p.x + lb * v[m].x, la * p.y + lb * v[m].y);
         ph[idx] = np;
         if constexpr (MODEL != MK_PLAIN) w[m] = cscale(np, ch);
+        if constexpr (MODEL == MK_ALUMINUM_G) pw[m] = cscale(np, a.tab_p[idx]);
       } else if constexpr (MODEL != MK_PLAIN) {
         w[m] = czero<C>();
       }
@@ -164,12 +169,20 @@ __global__ void __launch_bounds__(Width<Real>::W *(N / EE)) col_kernel(const Col
 #pragma unroll
           for (int m = 0; m < E; ++m) out[base + (long long)(j + T * m) * fs] = v[m];
         }
-        if constexpr (MODEL == MK_TUNGSTEN) {
+        if constexpr (MODEL == MK_TUNGSTEN || MODEL == MK_ALUMINUM_G) {
           C *out2 = reinterpret_cast<C *>(a.out[1]);
           fft_line_e<C, N, +1, N, E>(w, sm, ld, c, j, tw);
           if (ok) {
 #pragma unroll
             for (int m = 0; m < E; ++m) out2[base + (long long)(j + T * m) * fs] = w[m];
+          }
+        }
+        if constexpr (MODEL == MK_ALUMINUM_G) {
+          C *out3 = reinterpret_cast<C *>(a.out_p);
+          fft_line_e<C, N, +1, N, E>(pw, sm, ld, c, j, tw);
+          if (ok) {
+#pragma unroll
+            for (int m = 0; m < E; ++m) out3[base + (long long)(j + T * m) * fs] = pw[m];
           }
         }
       }
@@ -182,7 +195,7 @@ __global__ void __launch_bounds__(Width<Real>::W *(N / EE)) col_kernel(const Col
 // of length M of z[p] = x[2p] + i x[2p+1] and the split/merge post-processing.
 // ---------------------------------------------------------------------------
 template <typename Real> struct XArgs {
-  const void *in0, *in1;
+  const void *in0, *in1, *in2;
   void *out;
   const Real *rin;
   Real *rout;
@@ -192,6 +205,8 @@ template <typename Real> struct XArgs {
   double scale, mean;
   Real c0, c1, c2, c3, c4, c5;
   unsigned int *flag;
+  double al[18];  // MK_ALUMINUM_G coefficients (XLaunch::al)
+  const double *time;
 };
 
 // rows [row0, row0+W) of a split-layout complex array -> smem buf[k][c], k<=M
@@ -347,6 +362,46 @@ __global__ void __launch_bounds__(Width<Real>::W *(M / Plan<M>::E)) x_kernel(con
           bad |= !(isfinite(nx) && isfinite(ny));
           v[m] = mk<C>(nx, ny);
         }
+      } else if constexpr (MODEL == MK_ALUMINUM_G) {
+        // Aluminum.hpp:270-307: psi (u), psi_MF (v) and P*psi (q) in real space;
+        // moving temperature T_var(x, t); real cells 2p (re) and 2p + 1 (im)
+        C u[E];
+#pragma unroll
+        for (int m = 0; m < E; ++m) u[m] = v[m];
+        x_load_rows<C, M, W, NT>(reinterpret_cast<const C *>(a.in1), a.nyq_off, row0, a.rows, buf, tid);
+        __syncthreads();
+        x_pre<C, M, W, E>(buf, tw, c, j, v);
+        __syncthreads();
+        fft_line<C, M, +1, N0>(v, buf, ld, c, j, tw);
+        C q[E];
+        x_load_rows<C, M, W, NT>(reinterpret_cast<const C *>(a.in2), a.nyq_off, row0, a.rows, buf, tid);
+        __syncthreads();
+        x_pre<C, M, W, E>(buf, tw, c, j, q);
+        __syncthreads();
+        fft_line<C, M, +1, N0>(q, buf, ld, c, j, tw);
+        const double *al = a.al;
+        const double t = *a.time;
+        auto nl = [&](double x, Real uu, Real vv, Real qq) -> Real {
+          const double dist = x + al[3] - (x > al[4] ? al[2] : 0.0);
+          const double Tv = al[5] * (dist - al[6] - al[7] * t);
+          const Real q2N = (Real)(al[10] * Tv / al[8]);
+          const Real q3 = (Real)(al[12] * (al[9] + Tv) / al[8] + al[11]);
+          const Real kern = (Real)(-(1.0 - exp(-Tv / al[8]))) * qq;
+          return (Real)al[13] * uu * uu + (Real)al[14] * uu * uu * uu + q2N * vv + q3 * vv * vv +
+                 (Real)al[15] * vv * vv * vv - kern - (Real)al[16] * uu;
+        };
+#pragma unroll
+        for (int m = 0; m < E; ++m) {
+          const Real vx = to_real_plus_mean(v[m].x, a.scale, a.mean);
+          const Real vy = to_real_plus_mean(v[m].y, a.scale, a.mean);
+          const Real qx = to_real_plus_mean(q[m].x, a.scale, al[17] * a.mean);
+          const Real qy = to_real_plus_mean(q[m].y, a.scale, al[17] * a.mean);
+          const int i0 = 2 * (j + T * m);
+          const Real nx = nl(al[0] + i0 * al[1], u[m].x, vx, qx);
+          const Real ny = nl(al[0] + (i0 + 1) * al[1], u[m].y, vy, qy);
+          bad |= !(isfinite(nx) && isfinite(ny));
+          v[m] = mk<C>(nx, ny);
+        }
       } else if constexpr (MODEL == MK_FILTERED) {
         // N = p2 v^2/2 + p3 v^3/3 + p4 v^4/4 of the filtered density
 #pragma unroll
@@ -395,9 +450,12 @@ namespace opfc {
 // anti-Hermitian part, so it is removed from the resident state instead of
 // being left to grow under exp(L dt) > 1.
 template <typename Real>
-__global__ void herm_fix_kernel(typename Cx<Real>::T *psi, long long nyq_off, int M, int n1, int n2) {
+__global__ void herm_fix_kernel(typename Cx<Real>::T *psi, long long nyq_off, int M, int n1, int n2, double *time,
+                                double dt_time) {
   using C = typename Cx<Real>::T;
   const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  // the step's last kernel also advances the device time of the next step
+  if (time && e == 0 && blockIdx.y == 0) *time += dt_time;
   const long long plane = (long long)n1 * n2;
   if (e >= plane) return;
   const int y = (int)(e % n1), z = (int)(e / n1);
@@ -568,6 +626,8 @@ template <typename Real> static ColArgs<Real> col_args(const ColLaunch &L) {
   a.tab_a = reinterpret_cast<const Real *>(L.tab_a);
   a.tab_b = reinterpret_cast<const Real *>(L.tab_b);
   a.tab_chi = reinterpret_cast<const Real *>(L.tab_chi);
+  a.tab_p = reinterpret_cast<const Real *>(L.tab_p);
+  a.out_p = L.out_p;
   a.rad_ops = L.rad_ops;
   a.rad_chi = reinterpret_cast<const Real *>(L.rad_chi);
   a.rad_M = L.rad_M;
@@ -681,6 +741,9 @@ static int launch_col_n(const ColLaunch &L, cudaStream_t s) {
     case MK_FILTERED:
       return L.inverse_after ? launch_col_t<Real, N, COL_UPDATE, -1, MK_FILTERED, true>(L, s)
                              : launch_col_t<Real, N, COL_UPDATE, -1, MK_FILTERED, false>(L, s);
+    case MK_ALUMINUM_G:  // direct-load kernel, per-mode tables (opL, opN, chi, P_F)
+      if (!L.inverse_after) return (int)cudaErrorInvalidValue;
+      return launch_col_direct<Real, N, COL_UPDATE, -1, MK_ALUMINUM_G, true, OPS_TABLES>(L, s);
   }
   return (int)cudaErrorInvalidValue;
 }
@@ -689,6 +752,9 @@ template <typename Real> static XArgs<Real> x_args(const XLaunch &L) {
   XArgs<Real> a;
   a.in0 = L.in0;
   a.in1 = L.in1;
+  a.in2 = L.in2;
+  a.time = L.time;
+  for (int i = 0; i < 18; ++i) a.al[i] = L.al[i];
   a.out = L.out;
   a.rin = reinterpret_cast<const Real *>(L.rin);
   a.rout = reinterpret_cast<Real *>(L.rout);
@@ -762,6 +828,9 @@ static int launch_x_tma(const XLaunch &L, cudaStream_t s) {
     XArgs<Real> a;
     a.in0 = L.in0;
     a.in1 = L.in1;
+    a.in2 = L.in2;
+    a.time = L.time;
+    for (int i = 0; i < 18; ++i) a.al[i] = L.al[i];
     a.out = L.out;
     a.rin = nullptr;
     a.rout = nullptr;
@@ -800,6 +869,9 @@ static int launch_x_t(const XLaunch &L, cudaStream_t s) {
   XArgs<Real> a;
   a.in0 = L.in0;
   a.in1 = L.in1;
+  a.in2 = L.in2;
+  a.time = L.time;
+  for (int i = 0; i < 18; ++i) a.al[i] = L.al[i];
   a.out = L.out;
   a.rin = reinterpret_cast<const Real *>(L.rin);
   a.rout = reinterpret_cast<Real *>(L.rout);
@@ -866,6 +938,7 @@ static int launch_x_m(const XLaunch &L, cudaStream_t s) {
     case MK_PLAIN: return launch_x_t<Real, M, X_FUSED, MK_PLAIN>(L, s);
     case MK_TUNGSTEN: return launch_x_t<Real, M, X_FUSED, MK_TUNGSTEN>(L, s);
     case MK_FILTERED: return launch_x_t<Real, M, X_FUSED, MK_FILTERED>(L, s);
+    case MK_ALUMINUM_G: return launch_x_t<Real, M, X_FUSED, MK_ALUMINUM_G>(L, s);
   }
   return (int)cudaErrorInvalidValue;
 }
@@ -897,11 +970,12 @@ template <typename Real> int launch_x(const XLaunch &L, cudaStream_t s) {
 }
 
 template <typename Real>
-int launch_herm_fix(void *psi, long long nyq_off, int M, int n1, int n2, cudaStream_t s) {
+int launch_herm_fix(void *psi, long long nyq_off, int M, int n1, int n2, cudaStream_t s, double *time,
+                    double dt_time) {
   const long long plane = (long long)n1 * n2;
   dim3 grid((unsigned)((plane + 255) / 256), 2);
   herm_fix_kernel<Real><<<grid, 256, 0, s>>>(reinterpret_cast<typename Cx<Real>::T *>(psi), nyq_off,
-                                             M, n1, n2);
+                                             M, n1, n2, time, dt_time);
   return (int)cudaGetLastError();
 }
 
@@ -978,7 +1052,7 @@ int launch_energy_k(const void *psi_hat, int M, int n1, int n2, long long nyq_of
 #define OPFC_INSTANTIATE(R)                                                                          \
   template int launch_col<R>(const ColLaunch &, cudaStream_t);                                       \
   template int launch_x<R>(const XLaunch &, cudaStream_t);                                           \
-  template int launch_herm_fix<R>(void *, long long, int, int, int, cudaStream_t);                   \
+  template int launch_herm_fix<R>(void *, long long, int, int, int, cudaStream_t, double *, double);  \
   template int launch_to_ref<R>(const void *, void *, int, int, int, int, long long, int, double,    \
                                 cudaStream_t);                                                       \
   template int launch_from_ref<R>(const void *, int, void *, int, int, int, long long, cudaStream_t); \

@@ -29,7 +29,9 @@ struct ColSeg {
 };
 
 enum ColMode { COL_PLAIN = 0, COL_UPDATE = 1 };
-enum ModelKind { MK_PLAIN = 0, MK_TUNGSTEN = 1, MK_FILTERED = 2 };
+// MK_ALUMINUM_G: the Aluminum model with a moving temperature gradient (three
+// real fields per step: psi, psi_MF and P*psi; direct-load kernels only)
+enum ModelKind { MK_PLAIN = 0, MK_TUNGSTEN = 1, MK_FILTERED = 2, MK_ALUMINUM_G = 3 };
 
 struct ColLaunch {
   int N;        // transform length
@@ -48,6 +50,8 @@ struct ColLaunch {
   const void *tab_a;  // opL / exp_Ldt
   const void *tab_b;  // opN / n_weight
   const void *tab_chi;  // mean-field filter (TUNGSTEN, FILTERED)
+  const void *tab_p;    // MK_ALUMINUM_G: the correlation peak P_F
+  void *out_p;          // MK_ALUMINUM_G: inverse z transform of P_F psi_hat
   // TMA path (main segment): host CUtensorMap objects, see tma_col_width().
   // PLAIN: tmap[0], tmap[1] = input of array set 0 / 1; UPDATE: A, psi_hat,
   // tab_a, tab_b, tab_chi.  tmap[0] == nullptr selects the direct-load kernel.
@@ -97,6 +101,7 @@ struct XLaunch {
   long long nyq_off;
   const void *in0;   // complex input (split layout)
   const void *in1;   // second complex input (TUNGSTEN psi_MF)
+  const void *in2;   // third complex input (MK_ALUMINUM_G: P*psi)
   void *out;         // complex output (split layout)
   const void *rin;   // real rows (X_R2C)
   void *rout;        // real rows (X_C2R)
@@ -104,6 +109,13 @@ struct XLaunch {
   double scale;      // C2R normalisation 1/(N0 N1 N2)
   double mean;       // mean density added after the C2R (k = 0 mode in FP64)
   double c[8];       // nonlinearity coefficients
+  // MK_ALUMINUM_G: temperature T_var(x, t) = G (dist - x_init - V t) with
+  // dist = x + fullruns - (x > steppoint) l, x = x0 + i dx, t read from *time;
+  // N = p3b u^2 + p4b u^3 + q21b T/T0 v + (q31b (T_const + T)/T0 + q30b) v^2
+  //     + q4b v^3 + (1 - exp(-T/T0)) P*psi - stabP u
+  // (the mean of P*psi is P_F(0) times the mean density: PF0)
+  double al[18];       // x0 dx l fullruns steppoint G x_init V T0 T_const q21b q30b q31b p3b p4b q4b stabP PF0
+  const double *time;
   unsigned int *flag;  // bit 0: a non-finite value was produced; bit 1: a wait expired
   int use_tma;         // X_FUSED: persistent bulk-copy-fed kernel when the size allows
   int no_sq;           // X_FUSED: skip the warp-square kernel (x_sq.cuh) for x_tma.cuh
@@ -115,7 +127,8 @@ struct XLaunch {
 template <typename Real> int launch_col(const ColLaunch &a, cudaStream_t s);
 template <typename Real> int launch_x(const XLaunch &a, cudaStream_t s);
 template <typename Real>
-int launch_herm_fix(void *psi, long long nyq_off, int M, int n1, int n2, cudaStream_t s);
+int launch_herm_fix(void *psi, long long nyq_off, int M, int n1, int n2, cudaStream_t s,
+                    double *time = nullptr, double dt_time = 0.0);
 template <typename Real>
 int launch_to_ref(const void *in, void *out, int out_is_f64, int M, int n1, int n2,
                   long long nyq_off, int dc_override, double dc_re, cudaStream_t s);

@@ -100,6 +100,13 @@ struct opfc_handle {
   void *work_a = nullptr;    // F_z^-1 of the state, then the step's working array
   void *work_b = nullptr;    // TUNGSTEN: F_z^-1 of chi * state
   void *tab_a = nullptr, *tab_b = nullptr, *tab_chi = nullptr;
+  // Aluminum with a moving temperature gradient (G_grid != 0): the peak table
+  // P_F, F_z^-1[P_F psi_hat] between steps, and the device time of the next
+  // step (advanced by time_dt at the end of every step)
+  bool al_grad = false;
+  void *tab_p = nullptr, *work_c = nullptr;
+  double *time_dev = nullptr;
+  double time_dt = 0.0, pf0 = 0.0;
   void *tw_x = nullptr, *tw_y = nullptr, *tw_z = nullptr;
   void *real_buf = nullptr;  // real-space staging (N0 N1 N2 reals)
   unsigned int *flag = nullptr;
@@ -403,6 +410,10 @@ int prepare_a(opfc_handle *h) {
     int rc = opfc_scale_by_table(h, h->psi_hat, h->tab_chi, dst);
     if (rc) return rc;
     LAUNCH_TRY(h, col_plain(h, 2, +1, dst, dst));
+    if (h->al_grad) {  // P_F psi_hat -> C
+      if ((rc = opfc_scale_by_table(h, h->psi_hat, h->tab_p, h->work_c))) return rc;
+      LAUNCH_TRY(h, col_plain(h, 2, +1, h->work_c, h->work_c));
+    }
   }
   h->a_valid = true;
   return OPFC_OK;
@@ -417,10 +428,12 @@ const char *const kStepKernelNames[kStepKernels] = {"y_inverse", "x_fused", "y_f
 int enqueue_step(opfc_handle *h, int only = -1) {
   const int model = h->desc.model;
   if (only < 0 || only == 0) {  // YI
-    if (two_field(model))
+    if (two_field(model)) {
       LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_a, h->work_a, h->work_b, h->work_b));
-    else
+      if (h->al_grad) LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_c, h->work_c));
+    } else {
       LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_a, h->work_a));
+    }
   }
   if (only < 0 || only == 1) {  // X
     XLaunch X = x_base(h);
@@ -447,6 +460,18 @@ int enqueue_step(opfc_handle *h, int only = -1) {
       X.c[2] = p.q31_bar * p.T_const / p.T0 + p.q30_bar;
       X.c[3] = p.q4_bar;
       X.c[4] = p.stabP;
+      if (h->al_grad) {
+        // moving temperature: position- and time-dependent terms, third field
+        // P*psi (Aluminum.hpp:270-307); direct-load x kernel
+        X.model = MK_ALUMINUM_G;
+        X.in2 = h->work_c;
+        X.time = h->time_dev;
+        const double l = h->n0 * h->desc.dx[0];
+        const double al[18] = {h->desc.origin[0], h->desc.dx[0], l, std::floor(p.m_xpos / l) * l,
+                               std::fmod(p.m_xpos, l), p.G_grid, p.x_initial, p.V_grid, p.T0, p.T_const,
+                               p.q21_bar, p.q30_bar, p.q31_bar, p.p3_bar, p.p4_bar, p.q4_bar, p.stabP, h->pf0};
+        for (int i = 0; i < 18; ++i) X.al[i] = al[i];
+      }
     } else {
       X.model = MK_TUNGSTEN;
       X.in1 = h->work_b;
@@ -472,6 +497,11 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     col_segments(h, 2, Z);
     Z.mode = COL_UPDATE;
     Z.model = model == OPFC_MODEL_PLAIN ? MK_PLAIN : (two_field(model) ? MK_TUNGSTEN : MK_FILTERED);
+    if (h->al_grad) {  // three inverse transforms; direct-load kernel with per-mode tables
+      Z.model = MK_ALUMINUM_G;
+      Z.tab_p = h->tab_p;
+      Z.out_p = h->work_c;
+    }
     Z.inverse_after = 1;
     Z.nsets = 1;
     Z.in[0] = h->work_a;
@@ -496,7 +526,7 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.op_dt = h->dt;
     Z.op_chi = model == OPFC_MODEL_FILTERED ? 1.0 / (2.0 * h->desc.filter_alpha * h->desc.filter_alpha) : 0.0;
     const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE);
-    if (h->use_tma && h->var_z != 2 && h->var_z != 4 && Z.N > 1 && h->M % W == 0) {
+    if (h->use_tma && !h->al_grad && h->var_z != 2 && h->var_z != 4 && Z.N > 1 && h->M % W == 0) {
       Z.tmap[0] = tmap_for(h, h->work_a, 2, W, false);
       Z.tmap[1] = tmap_for(h, h->psi_hat, 2, W, false);
       if (Z.computed) {
@@ -520,9 +550,11 @@ int enqueue_step(opfc_handle *h, int only = -1) {
   }
   if (only < 0 || only == 4) {  // Hermitian projection of the kx = 0 / Nyquist planes
     if (h->prec == OPFC_FP64)
-      LAUNCH_TRY(h, launch_herm_fix<double>(h->psi_hat, h->nyq_off, h->M, h->n1, h->n2, h->stream));
+      LAUNCH_TRY(h, launch_herm_fix<double>(h->psi_hat, h->nyq_off, h->M, h->n1, h->n2, h->stream,
+                                            h->time_dev, h->time_dt));
     else
-      LAUNCH_TRY(h, launch_herm_fix<float>(h->psi_hat, h->nyq_off, h->M, h->n1, h->n2, h->stream));
+      LAUNCH_TRY(h, launch_herm_fix<float>(h->psi_hat, h->nyq_off, h->M, h->n1, h->n2, h->stream,
+                                           h->time_dev, h->time_dt));
   }
   return OPFC_OK;
 }
@@ -778,6 +810,19 @@ const char *opfc_status_string(int s) {
 
 const char *opfc_last_error(const opfc_handle *h) { return h ? h->err.c_str() : "null handle"; }
 
+int opfc_set_time(opfc_handle *h, double t, double dt_per_step) {
+  if (!h) return OPFC_ERR_ARG;
+  if (!h->time_dev) return OPFC_OK;  // the model's step does not depend on the time
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  CUDA_TRY(h, cudaMemcpyAsync(h->time_dev, &t, sizeof t, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+  if (h->time_dt != dt_per_step) {
+    h->time_dt = dt_per_step;
+    release_graph(h);  // the captured step bakes in the increment
+  }
+  return OPFC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // on-disk formats (io.h): the field goes through the host in FP64
 // ---------------------------------------------------------------------------
@@ -846,8 +891,8 @@ int opfc_destroy(opfc_handle *h) {
     if (p) cudaFree(p);
   for (void *p : h->seg)
     if (p) cudaFree(p);
-  void *adj[] = {h->tab_ar,   h->tab_br,   h->adj_c[0], h->adj_c[1], h->adj_r[0],
-                 h->adj_r[1], h->adj_r[2], h->rad_ops,  h->rad_chi};
+  void *adj[] = {h->tab_ar,   h->tab_br,   h->adj_c[0], h->adj_c[1], h->adj_r[0], h->adj_r[1],
+                 h->adj_r[2], h->rad_ops,  h->rad_chi,  h->tab_p,    h->work_c,   h->time_dev};
   for (void *p : adj)
     if (p) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -900,6 +945,12 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   if ((rc = dev_alloc(hp, &hp->psi_hat, cb))) return cleanup(rc);
   if ((rc = dev_alloc(hp, &hp->work_a, cb))) return cleanup(rc);
   if (two_field(d->model) && (rc = dev_alloc(hp, &hp->work_b, cb))) return cleanup(rc);
+  hp->al_grad = d->model == OPFC_MODEL_ALUMINUM && d->aluminum.G_grid != 0.0;
+  if (hp->al_grad) {
+    if ((rc = dev_alloc(hp, &hp->work_c, cb))) return cleanup(rc);
+    if ((rc = dev_alloc(hp, (void **)&hp->time_dev, sizeof(double)))) return cleanup(rc);
+    if (cudaMemset(hp->time_dev, 0, sizeof(double)) != cudaSuccess) return cleanup(OPFC_ERR_CUDA);
+  }
   if ((rc = upload_twiddles(hp, hp->n0, &hp->tw_x))) return cleanup(rc);
   if ((rc = upload_twiddles(hp, hp->n1, &hp->tw_y))) return cleanup(rc);
   if ((rc = upload_twiddles(hp, hp->n2, &hp->tw_z))) return cleanup(rc);
@@ -940,34 +991,36 @@ int opfc_initialize(opfc_handle *h, double dt) {
   const double r = h->desc.r;
   const double fa = h->desc.filter_alpha;
   const opfc_aluminum_params A = h->desc.aluminum;
-  if (model == OPFC_MODEL_ALUMINUM) {
-    if (A.G_grid != 0.0)
-      return fail(h, OPFC_ERR_ARG,
-                  "Aluminum: a moving temperature gradient (G_grid != 0) is not available on this path");
-    if (A.T0 == 0.0) return fail(h, OPFC_ERR_ARG, "Aluminum: T0 must be nonzero");
-  }
+  if (model == OPFC_MODEL_ALUMINUM && A.T0 == 0.0) return fail(h, OPFC_ERR_ARG, "Aluminum: T0 must be nonzero");
   // Aluminum.hpp:186-242 (prepare_operators): chi = exp(kLap/(2 lambda^2)); the
   // peak is the larger of the Gaussians around |k| = 1 and 2/sqrt(3);
   // P_F = Bx exp(-tau_const) peak; opCk = stabP + p2_bar - P_F + q2_bar_L chi;
   // opL = exp(kLap opCk dt); opN = kLap dt if opCk == 0 else (opL - 1)/opCk
-  auto aluminum_mode = [&](double kLap, double &oa, double &ob, double &oc) {
-    const double a2 = 2.0 * A.alpha * A.alpha, l2 = 2.0 * A.lambda * A.lambda;
-    const double fMF = std::exp(kLap / l2);
+  auto aluminum_peak = [&](double kLap) {
+    const double a2 = 2.0 * A.alpha * A.alpha;
     const double kw = std::sqrt(-kLap) - 1.0, kp = std::sqrt(-kLap) - 2.0 / std::sqrt(3.0);
     const double g1 = std::exp(-(kw * kw) / a2), gp1 = std::exp(-(kp * kp) / a2);
-    const double PF = A.Bx * std::exp(-A.tau_const) * (g1 > gp1 ? g1 : gp1);
+    return A.Bx * std::exp(-A.tau_const) * (g1 > gp1 ? g1 : gp1);
+  };
+  auto aluminum_mode = [&](double kLap, double &oa, double &ob, double &oc) {
+    const double l2 = 2.0 * A.lambda * A.lambda;
+    const double fMF = std::exp(kLap / l2);
+    const double PF = aluminum_peak(kLap);
     const double opCk = A.stabP + A.p2_bar - PF + A.q2_bar_L * fMF;
     oa = std::exp(kLap * opCk * dt);
     ob = (opCk == 0.0) ? kLap * dt : (oa - 1.0) / opCk;
     oc = fMF;
   };
+  std::vector<double> tp(h->al_grad ? h->nc : 0);
   parallel_for((long)n2 * n1, [&](long row) {
     const int ky = (int)(row % n1), kz = (int)(row / n1);
     for (int kx = 0; kx < H; ++kx) {
       const double kx_ = kc(kx, n0, f0), ky_ = kc(ky, n1, f1), kz_ = kc(kz, n2, f2);
       const size_t o = split_index(h, kx, ky, kz);
       if (model == OPFC_MODEL_ALUMINUM) {
-        aluminum_mode(-((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_)), ta[o], tb[o], tc[o]);
+        const double kLap = -((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_));
+        aluminum_mode(kLap, ta[o], tb[o], tc[o]);
+        if (h->al_grad) tp[o] = aluminum_peak(kLap);
       } else if (model == OPFC_MODEL_TUNGSTEN) {
         // physics_for_mode (tungsten_spectral.hpp:83-104) + spectral_exp_coeffs
         // (spectral_exp_coefficients.hpp:68-82) + n_weight (tungsten_etd_workspace.hpp:111-130)
@@ -1016,13 +1069,19 @@ int opfc_initialize(opfc_handle *h, double dt) {
   if ((rc = upload(ta, &h->tab_a))) return rc;
   if ((rc = upload(tb, &h->tab_b))) return rc;
   if (need_chi && (rc = upload(tc, &h->tab_chi))) return rc;
+  if (h->al_grad) {
+    if ((rc = upload(tp, &h->tab_p))) return rc;
+    h->pf0 = aluminum_peak(0.0);
+    h->time_dt = dt;
+    CUDA_TRY(h, cudaMemset(h->time_dev, 0, sizeof(double)));
+  }
 
   // Isotropic grids (one frequency step f on all axes): every operator depends
   // only on m = i^2 + j^2 + k^2 of the folded integer indices (k^2 = f^2 m), so
   // the fused z update reads small L2-resident tables instead of streaming the
   // per-mode tables from HBM.  Same formulas, FP64, rounded once.
   const char *no_rad = std::getenv("OPFC_NO_RADIAL");
-  if (f0 == f1 && f1 == f2 && !(no_rad && no_rad[0] == '1')) {
+  if (f0 == f1 && f1 == f2 && !(no_rad && no_rad[0] == '1') && !h->al_grad) {
     const long mmax = (long)(n0 / 2) * (n0 / 2) + (long)(n1 / 2) * (n1 / 2) + (long)(n2 / 2) * (n2 / 2);
     const size_t cnt = (size_t)mmax + 1;
     std::vector<double> ops(2 * cnt), chi(need_chi ? cnt : 0);

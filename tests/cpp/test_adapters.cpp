@@ -22,6 +22,7 @@ static int failures = 0;
     if (!(cond)) {                        \
       std::printf("FAIL: " __VA_ARGS__);  \
       std::printf("\n");                  \
+      std::fflush(stdout);                \
       ++failures;                         \
     }                                     \
   } while (0)

@@ -63,9 +63,26 @@ def test_aluminum_larger_grid_vs_oracle(oracle):
     assert np.linalg.norm((m.get_psi() - ref).ravel()) <= 1e-11 * np.linalg.norm(ref.ravel())
 
 
-def test_aluminum_moving_gradient_refused():
-    p = params()
-    p.G_grid = 1.0
-    m = ob.AluminumB200((16, 16, 16), [1.0] * 3, p)
-    with pytest.raises(ob.OpfcError):
-        m.initialize(1e-2)
+@pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
+def test_aluminum_moving_gradient_vs_oracle(oracle, prec, tol):
+    # G_grid != 0: T_var(x, t) = G (dist - x_initial - V t) with the wrap at
+    # m_xpos, a third field P*psi, time t0 + s dt for step s (Aluminum.hpp:262-307)
+    vals = dict(G_grid=2.0, V_grid=0.5, q4_bar=0.787482, tau_const=0.3, m_xpos=5.0, x_initial=4.0, stabP=0.05)
+    p, op = params(), oracle.AluminumParams.test_case()
+    for k, v in vals.items():
+        setattr(p, k, v)
+        setattr(op, k, v)
+    origin = [-3.0, 0.0, 0.0]
+    psi0 = ic()
+    m = ob.AluminumB200((32, 32, 32), [1.0] * 3, p, precision=prec, origin=origin)
+    m.initialize(1e-2)
+    m.set_psi(psi0)
+    m.set_time(0.3, 1e-2)
+    m.step(4)
+    m.sync()
+    ref = oracle.run_aluminum(psi0, [1.0] * 3, origin, op, 1e-2, 4, t0=0.3, dt_t=1e-2)
+    got = m.get_psi()
+    assert np.linalg.norm((got - ref).ravel()) <= tol * np.linalg.norm(ref.ravel())
+    # the gradient acts: without it the result differs
+    base = oracle.run_aluminum(psi0, [1.0] * 3, origin, oracle.AluminumParams.test_case(), 1e-2, 4, t0=0.3)
+    assert np.abs(ref - base).max() > 1e-6
