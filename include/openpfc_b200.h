@@ -45,6 +45,7 @@ extern "C" {
 #define OPFC_MODEL_TUNGSTEN 1  /* Tungsten ETD, apps/tungsten/include/tungsten/cpu/tungsten_model.hpp:306-366 */
 #define OPFC_MODEL_FILTERED 2  /* Gaussian mean-field filter + polynomial of psi_MF */
 #define OPFC_MODEL_ALUMINUM 3  /* Aluminum PFC variant, apps/aluminumNew/Aluminum.hpp */
+#define OPFC_MODEL_USER_ETD 4  /* caller-supplied ETD1 operators (opfc_set_operators) */
 
 /* where a user pointer lives */
 #define OPFC_HOST 0
@@ -221,6 +222,18 @@ int opfc_set_r(opfc_handle *h, double r);
  * advances it by dt_per_step on the device (opfc_initialize sets the time to 0
  * and the increment to dt).  Other models ignore it. */
 int opfc_set_time(opfc_handle *h, double t, double dt_per_step);
+/* OPFC_MODEL_USER_ETD: the GPU backend of the reference's generic ETD1 stepper
+ * (Etd1Stepper::set_coefficients / attempt_step,
+ * include/openpfc/kernel/simulation/steppers/etd1.hpp, with the spectral
+ * coefficients of spectral_exp_coefficients.hpp): per-mode tables in the
+ * reference's half-spectrum layout ((N0/2+1) x N1 x N2, count entries):
+ * psi_hat <- exp_Ldt psi_hat + n_weight N_hat with N = p2 v^2/2 + p3 v^3/3 +
+ * p4 v^4/4 (opfc_desc p2, p3, p4) of v = F^-1[chi psi_hat] (chi NULL = 1).
+ * The fused passes carry the mean exactly, so the k = 0 entries must be
+ * exp_Ldt = 1, n_weight = 0, chi = 1 (conserved dynamics), else OPFC_ERR_ARG.
+ * Call before opfc_initialize (whose dt is then only recorded). */
+int opfc_set_operators(opfc_handle *h, const double *exp_Ldt, const double *n_weight, const double *chi,
+                       size_t count);
 int opfc_forward_checkpointed(opfc_handle *h, int n_steps, int K);
 int opfc_adjoint(opfc_handle *h, const void *grad_psi_T, int dtype, int where, void *grad_psi0,
                  double *grad_r, double *grad_n0);

@@ -23,9 +23,10 @@ import numpy as np
 
 from . import _lib
 from ._lib import (DEVICE, F32, F64, FP32, FP64, HOST, MODEL_ALUMINUM, MODEL_FILTERED, MODEL_PLAIN,
-                   MODEL_TUNGSTEN, AluminumParams, Desc, OpfcError, TungstenParams, default_desc, lib)
+                   MODEL_TUNGSTEN, MODEL_USER_ETD, AluminumParams, Desc, OpfcError, TungstenParams,
+                   default_desc, lib)
 
-__all__ = ["B200Fft", "PfcB200", "TungstenB200", "FilteredB200", "AluminumB200", "AluminumParams", "Desc",
+__all__ = ["B200Fft", "PfcB200", "TungstenB200", "FilteredB200", "AluminumB200", "AluminumParams", "EtdB200", "Desc",
            "TungstenParams",
            "OpfcError", "default_desc", "lib", "FP32", "FP64"]
 
@@ -339,6 +340,31 @@ class AluminumB200(_ModelBase):
         if params is not None:
             d.aluminum = params
         super().__init__(d)
+
+
+class EtdB200(_ModelBase):
+    """Caller-supplied ETD1 operators on the fused passes (the GPU backend of the
+    reference's Etd1Stepper, include/openpfc/kernel/simulation/steppers/etd1.hpp):
+    psi_hat <- exp_Ldt psi_hat + n_weight F[N], N = p2 v^2/2 + p3 v^3/3 + p4 v^4/4
+    of v = F^-1[chi psi_hat].  set_operators() takes arrays of the reference's
+    half-spectrum shape (N2, N1, N0//2+1); k = 0 must conserve the mean."""
+
+    def __init__(self, n, dx, p2: float = 0.0, p3: float = 0.0, p4: float = 0.0, precision: int = FP64,
+                 device: int = 0, origin=None, stream=None):
+        d = default_desc()
+        _geom(d, n, dx, origin, precision, device, stream)
+        d.model = MODEL_USER_ETD
+        d.p2, d.p3, d.p4 = float(p2), float(p3), float(p4)
+        self._nc = (int(n[0]) // 2 + 1) * int(n[1]) * int(n[2])
+        super().__init__(d)
+
+    def set_operators(self, exp_Ldt, n_weight, chi=None):
+        a = np.ascontiguousarray(exp_Ldt, dtype=np.float64).ravel()
+        b = np.ascontiguousarray(n_weight, dtype=np.float64).ravel()
+        c = None if chi is None else np.ascontiguousarray(chi, dtype=np.float64).ravel()
+        dp = ctypes.POINTER(ctypes.c_double)
+        _check(self._h, lib().opfc_set_operators(self._h, a.ctypes.data_as(dp), b.ctypes.data_as(dp),
+                                                 None if c is None else c.ctypes.data_as(dp), a.size))
 
 
 # ---------------------------------------------------------------------------

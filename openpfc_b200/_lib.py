@@ -18,7 +18,7 @@ STATUS = {0: "OPFC_OK", -1: "OPFC_ERR_ARG", -2: "OPFC_ERR_SIZE", -3: "OPFC_ERR_C
           -4: "OPFC_ERR_NONFINITE", -5: "OPFC_ERR_TIMEOUT", -6: "OPFC_ERR_OOM",
           -7: "OPFC_ERR_STATE", -8: "OPFC_ERR_IO"}
 FP32, FP64 = 0, 1
-MODEL_PLAIN, MODEL_TUNGSTEN, MODEL_FILTERED, MODEL_ALUMINUM = 0, 1, 2, 3
+MODEL_PLAIN, MODEL_TUNGSTEN, MODEL_FILTERED, MODEL_ALUMINUM, MODEL_USER_ETD = 0, 1, 2, 3, 4
 HOST, DEVICE = 0, 1
 F32, F64 = 0, 1
 
@@ -125,6 +125,7 @@ def lib():
     L.opfc_read_binary.argtypes = [H, cp]
     L.opfc_write_vti.argtypes = [H, cp, ci, cp]
     L.opfc_set_time.argtypes = [H, cd, cd]
+    L.opfc_set_operators.argtypes = [H, dp, dp, dp, sz]
     L.opfc_write_raw.argtypes = [cp, ip, ip, ip, dp, ci]
     L.opfc_read_raw.argtypes = [cp, ip, ip, ip, dp, ci]
     L.opfc_write_vti_raw.argtypes = [cp, ip, ip, ip, dp, dp, cp, dp]

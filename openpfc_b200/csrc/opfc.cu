@@ -39,7 +39,9 @@ namespace {
 constexpr double kPi = 3.14159265358979323846264338327950288;
 constexpr int kVarY = 5, kVarX = 4, kVarZ = 6;
 // models with two real fields per step (psi and psi_MF): Tungsten, Aluminum
-inline bool two_field(int model) { return model == OPFC_MODEL_TUNGSTEN || model == OPFC_MODEL_ALUMINUM; }  // kernel variants per pass (opfc_autotune)
+inline bool two_field(int model) { return model == OPFC_MODEL_TUNGSTEN || model == OPFC_MODEL_ALUMINUM; }
+// operator tables supplied by the caller (opfc_set_operators), filtered-model passes
+inline bool user_ops_model(int model) { return model == OPFC_MODEL_USER_ETD; }  // kernel variants per pass (opfc_autotune)
 
 bool supported_len(int n) {
   static const int ok[] = {1, 2, 4, 8, 16, 24, 32, 40, 48, 64, 80, 96, 128, 256, 512, 1024};
@@ -104,6 +106,7 @@ struct opfc_handle {
   // P_F, F_z^-1[P_F psi_hat] between steps, and the device time of the next
   // step (advanced by time_dt at the end of every step)
   bool al_grad = false;
+  bool user_ops = false;  // OPFC_MODEL_USER_ETD: tables set by opfc_set_operators
   void *tab_p = nullptr, *work_c = nullptr;
   double *time_dev = nullptr;
   double time_dt = 0.0, pf0 = 0.0;
@@ -443,7 +446,7 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     X.mean = mean_density(h);
     if (model == OPFC_MODEL_PLAIN) {
       X.model = MK_PLAIN;
-    } else if (model == OPFC_MODEL_FILTERED) {
+    } else if (model == OPFC_MODEL_FILTERED || user_ops_model(model)) {
       X.model = MK_FILTERED;
       X.c[0] = h->desc.p2 / 2.0;
       X.c[1] = h->desc.p3 / 3.0;
@@ -515,7 +518,7 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.tab_chi = h->tab_chi;
     Z.axis = 2;
     // computed operators (variants 3, 4): PLAIN and FILTERED models
-    Z.computed = h->var_z >= 3 && !two_field(model);
+    Z.computed = h->var_z >= 3 && !two_field(model) && !user_ops_model(model);
     Z.pingpong = h->var_z == 5;
     Z.rad_M = h->M;
     Z.rad_n1 = h->n1;
@@ -810,6 +813,44 @@ const char *opfc_status_string(int s) {
 
 const char *opfc_last_error(const opfc_handle *h) { return h ? h->err.c_str() : "null handle"; }
 
+int opfc_set_operators(opfc_handle *h, const double *exp_Ldt, const double *n_weight, const double *chi,
+                       size_t count) {
+  if (!h || !exp_Ldt || !n_weight) return h ? fail(h, OPFC_ERR_ARG, "null operator table") : OPFC_ERR_ARG;
+  if (!user_ops_model(h->desc.model)) return fail(h, OPFC_ERR_ARG, "opfc_set_operators: not a user ETD model");
+  int rc;
+  if ((rc = check_count(h, count, h->nc, "opfc_set_operators"))) return rc;
+  // the mean is carried exactly on the host: the operators must conserve it
+  if (std::fabs(exp_Ldt[0] - 1.0) > 1e-12 || n_weight[0] != 0.0 || (chi && std::fabs(chi[0] - 1.0) > 1e-12))
+    return fail(h, OPFC_ERR_ARG,
+                "opfc_set_operators: k = 0 must have exp_Ldt = 1, n_weight = 0, chi = 1 (conserved dynamics)");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  const int H = h->M + 1;
+  std::vector<double> t[3] = {std::vector<double>(h->nc), std::vector<double>(h->nc), std::vector<double>(h->nc)};
+  const double *src[3] = {exp_Ldt, n_weight, chi};
+  parallel_for((long)h->n2 * h->n1, [&](long row) {
+    const int ky = (int)(row % h->n1), kz = (int)(row / h->n1);
+    for (int kx = 0; kx < H; ++kx) {
+      const size_t r = (size_t)kx + (size_t)H * (size_t)row;  // reference layout
+      const size_t o = split_index(h, kx, ky, kz);
+      for (int q = 0; q < 3; ++q) t[q][o] = src[q] ? src[q][r] : 1.0;
+    }
+  });
+  void **dst[3] = {&h->tab_a, &h->tab_b, &h->tab_chi};
+  for (int q = 0; q < 3; ++q) {
+    if (!*dst[q] && (rc = dev_alloc(h, dst[q], h->nc * h->rsz))) return rc;
+    if (h->prec == OPFC_FP64) {
+      CUDA_TRY(h, cudaMemcpy(*dst[q], t[q].data(), h->nc * 8, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(t[q].begin(), t[q].end());
+      CUDA_TRY(h, cudaMemcpy(*dst[q], f.data(), h->nc * 4, cudaMemcpyHostToDevice));
+    }
+  }
+  h->user_ops = true;
+  h->a_valid = false;
+  release_graph(h);
+  return OPFC_OK;
+}
+
 int opfc_set_time(opfc_handle *h, double t, double dt_per_step) {
   if (!h) return OPFC_ERR_ARG;
   if (!h->time_dev) return OPFC_OK;  // the model's step does not depend on the time
@@ -907,7 +948,7 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   std::unique_ptr<opfc_handle> h(new opfc_handle);
   h->desc = *d;
   if (d->precision != OPFC_FP32 && d->precision != OPFC_FP64) return OPFC_ERR_ARG;
-  if (d->model < OPFC_MODEL_PLAIN || d->model > OPFC_MODEL_ALUMINUM) return OPFC_ERR_ARG;
+  if (d->model < OPFC_MODEL_PLAIN || d->model > OPFC_MODEL_USER_ETD) return OPFC_ERR_ARG;
   for (int a = 0; a < 3; ++a)
     if (d->n[a] < 1 || !(d->dx[a] > 0)) return OPFC_ERR_SIZE;
   if (d->n[0] < 2 || d->n[0] % 2 != 0) return OPFC_ERR_SIZE;
@@ -965,10 +1006,17 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   return OPFC_OK;
 }
 
+static int finish_initialize(opfc_handle *h);
+
 int opfc_initialize(opfc_handle *h, double dt) {
   if (!h) return OPFC_ERR_ARG;
   if (!(dt > 0) || !std::isfinite(dt)) return fail(h, OPFC_ERR_ARG, "dt must be positive and finite");
   CUDA_TRY(h, cudaSetDevice(h->device));
+  if (user_ops_model(h->desc.model)) {  // the caller's tables already include dt
+    if (!h->user_ops) return fail(h, OPFC_ERR_STATE, "user ETD model: call opfc_set_operators first");
+    h->dt = dt;
+    return finish_initialize(h);
+  }
   const int n0 = h->n0, n1 = h->n1, n2 = h->n2, H = h->M + 1;
   const double f0 = 2.0 * kPi / (h->desc.dx[0] * n0);
   const double f1 = 2.0 * kPi / (h->desc.dx[1] * n1);
@@ -1130,6 +1178,12 @@ int opfc_initialize(opfc_handle *h, double dt) {
     if (need_chi && (rc = up(chi, &h->rad_chi))) return rc;
   }
   h->dt = dt;
+  return finish_initialize(h);
+}
+
+// kernel variants and handle state after the operator tables exist
+static int finish_initialize(opfc_handle *h) {
+  const int model = h->desc.model;
   // kernel variants: the autotuner's cached choice, else the defaults;
   // OPFC_Y_VARIANT / OPFC_X_VARIANT / OPFC_Z_VARIANT force a pass's variant
   h->var_y = AutoTuner::instance().get_config(tune_key(h, "y"), 0);
@@ -1140,7 +1194,7 @@ int opfc_initialize(opfc_handle *h, double dt) {
   if (const char *xv = std::getenv("OPFC_X_VARIANT")) h->var_x = std::atoi(xv);
   if (h->var_x < 0 || h->var_x >= kVarX) h->var_x = 0;
   if (h->var_z == 1 && !h->rad_ops) h->var_z = 0;
-  if (h->var_z >= 3 && two_field(model)) h->var_z = h->var_z == 4 ? 2 : 0;
+  if (h->var_z >= 3 && (two_field(model) || user_ops_model(model))) h->var_z = h->var_z == 4 ? 2 : 0;
   if (h->var_z < 0 || h->var_z >= kVarZ) h->var_z = 0;
   if (h->var_y < 0 || h->var_y >= kVarY) h->var_y = 0;
   h->initialized = true;
@@ -1318,7 +1372,7 @@ int opfc_mass(opfc_handle *h, double *mean) {
 int opfc_free_energy(opfc_handle *h, double *energy) {
   if (!h || !energy) return OPFC_ERR_ARG;
   if (!h->have_state) return fail(h, OPFC_ERR_STATE, "no state");
-  if (two_field(h->desc.model))
+  if (two_field(h->desc.model) || user_ops_model(h->desc.model))
     return fail(h, OPFC_ERR_ARG, "free energy is defined for the plain and filtered models");
   CUDA_TRY(h, cudaSetDevice(h->device));
   // quadratic part by Parseval in k-space (FP64 accumulation of the resident state)
@@ -1366,7 +1420,7 @@ int opfc_autotune(opfc_handle *h, double *ms) {
       tune_key(h, "z"), kVarZ,
       [&](int v) {
         if (v == 1 && !h->rad_ops) return (int)OPFC_ERR_ARG;
-        if (v >= 3 && two_field(h->desc.model)) return (int)OPFC_ERR_ARG;
+        if (v >= 3 && (two_field(h->desc.model) || user_ops_model(h->desc.model))) return (int)OPFC_ERR_ARG;
         h->var_z = v;
         return enqueue_step(h, 3);
       },
@@ -1790,7 +1844,8 @@ extern "C" {
 
 int opfc_set_r(opfc_handle *h, double r) {
   if (!h) return OPFC_ERR_ARG;
-  if (two_field(h->desc.model)) return fail(h, OPFC_ERR_ARG, "r is not a parameter of this model");
+  if (two_field(h->desc.model) || user_ops_model(h->desc.model))
+    return fail(h, OPFC_ERR_ARG, "r is not a parameter of this model");
   h->desc.r = r;
   release_graph(h);
   h->ckpt_steps = 0;
