@@ -1404,7 +1404,8 @@ size_t opfc_size_inbox(const opfc_handle *h) { return h ? h->nr : 0; }
 size_t opfc_size_outbox(const opfc_handle *h) { return h ? h->nc : 0; }
 size_t opfc_allocated_bytes(const opfc_handle *h) { return h ? h->allocated : 0; }
 void *opfc_get_stream(const opfc_handle *h) { return h ? (void *)h->stream : nullptr; }
-int opfc_kernels_per_step(const opfc_handle *h) { return h ? kStepKernels : 0; }
+// (the Aluminum gradient model's y pass launches once more, for P*psi)
+int opfc_kernels_per_step(const opfc_handle *h) { return h ? kStepKernels + (h->al_grad ? 1 : 0) : 0; }
 
 int opfc_autotune(opfc_handle *h, double *ms) {
   if (!h) return OPFC_ERR_ARG;
