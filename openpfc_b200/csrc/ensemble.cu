@@ -361,7 +361,13 @@ int opfc_ensemble_create(int count, const opfc_desc *descs, opfc_ensemble **out)
         return bail(OPFC_ERR_CUDA);
     }
   }
-  if (cudaMemset(ep->flag, 0, sizeof(unsigned)) != cudaSuccess || cudaMemset(ep->psi_hat, 0, cb) != cudaSuccess)
+  if (cudaMemset(ep->flag, 0, sizeof(unsigned)) != cudaSuccess || cudaMemset(ep->psi_hat, 0, cb) != cudaSuccess ||
+      cudaMemset(ep->work, 0, cb) != cudaSuccess)
+    return bail(OPFC_ERR_CUDA);
+  // every instance's descriptor is on the device from the start (set_psi
+  // refreshes its mean), so the stage kernels -- and the autotuner timing
+  // them before any state is set -- walk every member's tiles
+  if (cudaMemcpy(ep->d_inst, ep->inst.data(), sizeof(EnsInst) * count, cudaMemcpyHostToDevice) != cudaSuccess)
     return bail(OPFC_ERR_CUDA);
   // dynamic shared memory above 48 KB is never needed (N <= 128)
   ep->var_col = AutoTuner::instance().get_config(ep->key + "/col", 0);
