@@ -200,7 +200,9 @@ int opfc_variants(const opfc_handle *h, int *var);
  * one precision.  Every stage of a step is one persistent kernel over all
  * members; opfc_ensemble_step(n) captures the n-step loop as one CUDA graph.
  * Fields are host FP64 arrays (x fastest).  opfc_ensemble_autotune times the
- * tile-shape variants of the column and x stages, caches the fastest (see
+ * variants (tile width 16 / 8 lines x 4 / 8 / 16 CTAs per SM, which also sets
+ * the kernel's register budget) of the y, x and z-update stages separately,
+ * reports 6 milliseconds per stage, caches the fastest (see
  * OPENPFC_GPU_AUTOTUNE_* in the library notes) and invalidates the states. */
 typedef struct opfc_ensemble opfc_ensemble;
 int opfc_ensemble_create(int count, const opfc_desc *descs, opfc_ensemble **out);
@@ -211,8 +213,8 @@ int opfc_ensemble_set_psi(opfc_ensemble *e, int member, const double *psi, size_
 int opfc_ensemble_get_psi(opfc_ensemble *e, int member, double *psi, size_t count);
 int opfc_ensemble_step(opfc_ensemble *e, int n_steps);
 int opfc_ensemble_sync(opfc_ensemble *e);
-int opfc_ensemble_autotune(opfc_ensemble *e, double *ms_col, double *ms_x);
-int opfc_ensemble_variants(const opfc_ensemble *e, int *var_col, int *var_x);
+int opfc_ensemble_autotune(opfc_ensemble *e, double *ms_col, double *ms_x, double *ms_upd);
+int opfc_ensemble_variants(const opfc_ensemble *e, int *var_col, int *var_x, int *var_upd);
 size_t opfc_ensemble_cells(const opfc_ensemble *e);
 void *opfc_ensemble_stream(const opfc_ensemble *e);
 

@@ -497,15 +497,18 @@ class Ensemble:
         self._check(lib().opfc_ensemble_sync(self._h))
 
     def autotune(self):
-        """Time the tile-shape variants, keep the fastest; states must be set again."""
-        mc, mx = (ctypes.c_double * 6)(), (ctypes.c_double * 6)()
-        self._check(lib().opfc_ensemble_autotune(self._h, mc, mx))
-        return list(mc), list(mx)
+        """Time the tile-shape / occupancy variants of the y, x and z-update
+        stages, keep the fastest of each; states must be set again.  Returns
+        the milliseconds per variant: (y, x, z update)."""
+        mc, mx, mu = (ctypes.c_double * 6)(), (ctypes.c_double * 6)(), (ctypes.c_double * 6)()
+        self._check(lib().opfc_ensemble_autotune(self._h, mc, mx, mu))
+        return list(mc), list(mx), list(mu)
 
     def variants(self):
-        a, b = ctypes.c_int(), ctypes.c_int()
-        self._check(lib().opfc_ensemble_variants(self._h, ctypes.byref(a), ctypes.byref(b)))
-        return a.value, b.value
+        """Chosen variants (y passes, x pass, z update)."""
+        a, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(lib().opfc_ensemble_variants(self._h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
 
     @property
     def cells(self) -> int:

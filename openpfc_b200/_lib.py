@@ -138,8 +138,8 @@ def lib():
     L.opfc_ensemble_get_psi.argtypes = [H, ci, dp, sz]
     L.opfc_ensemble_step.argtypes = [H, ci]
     L.opfc_ensemble_sync.argtypes = [H]
-    L.opfc_ensemble_autotune.argtypes = [H, dp, dp]
-    L.opfc_ensemble_variants.argtypes = [H, ip, ip]
+    L.opfc_ensemble_autotune.argtypes = [H, dp, dp, dp]
+    L.opfc_ensemble_variants.argtypes = [H, ip, ip, ip]
     L.opfc_ensemble_cells.argtypes = [H]
     L.opfc_ensemble_cells.restype = sz
     L.opfc_ensemble_stream.argtypes = [H]

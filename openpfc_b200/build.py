@@ -21,7 +21,8 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libopenpfc_b200.so")
-SOURCES = ["kernels_f32.cu", "kernels_f64.cu", "opfc.cu", "noalloc.cu", "ensemble.cu", "io.cu"]
+SOURCES = ["kernels_f32.cu", "kernels_f64.cu", "ensemble_f32.cu", "ensemble_f64.cu", "opfc.cu", "noalloc.cu",
+           "ensemble.cu", "io.cu"]
 HEADERS = ["fft_core.cuh", "kernels.cuh", "launch.h", "col_tma.cuh", "x_tma.cuh", "x_sq.cuh", "twiddle.h",
            "ensemble.cuh", "autotune.h", "io.h"]
 
@@ -45,12 +46,24 @@ def _stale(target: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _deps(obj: str, src: str):
+    """Headers the object was built from (nvcc -MD file), else every header."""
+    dfile = obj[:-2] + ".d"
+    if os.path.exists(dfile):
+        with open(dfile) as f:
+            text = f.read().replace("\\\n", " ")
+        files = [t for t in text.split(":", 1)[-1].split() if t.startswith(ROOT)]
+        if files and all(os.path.exists(t) for t in files):
+            return files
+    return [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS] + \
+        [os.path.join(ROOT, "include", "openpfc_b200.h")]
+
+
 def _compile(src: str, extra) -> str:
     obj = os.path.join(BUILD, os.path.splitext(src)[0] + ".o")
-    deps = [os.path.join(CSRC, src)] + [os.path.join(CSRC, h) for h in HEADERS] + \
-        [os.path.join(ROOT, "include", "openpfc_b200.h")]
-    if _stale(obj, deps):
-        cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ["-c", os.path.join(CSRC, src), "-o", obj]
+    if _stale(obj, _deps(obj, src)):
+        cmd = [nvcc()] + NVCC_FLAGS + list(extra) + ["-MD", "-MF", obj[:-2] + ".d",
+                                                     "-c", os.path.join(CSRC, src), "-o", obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")

@@ -45,14 +45,14 @@ struct opfc_ensemble {
   double dt = 0;
   bool initialized = false, a_valid = false;
   std::vector<bool> have_state;
-  void *psi_hat = nullptr, *work = nullptr, *tab_a = nullptr, *tab_b = nullptr, *tw = nullptr;
+  void *psi_hat = nullptr, *work = nullptr, *tw = nullptr;
   void *real_buf = nullptr;
   EnsInst *d_inst = nullptr;
   int *d_prefix[3] = {nullptr, nullptr, nullptr};  // y col, z col, x tiles (per W variant)
   int total[2][3] = {};                           // [W = 16, 8][stage]
   int *d_prefix8[3] = {nullptr, nullptr, nullptr};
   unsigned *flag = nullptr;
-  int var_col = 0, var_x = 0;
+  int var_col = 0, var_x = 0, var_upd = 0;  // y passes, x pass, z update
   cudaGraphExec_t graph = nullptr;
   int graph_steps = 0;
   std::string err;
@@ -100,52 +100,28 @@ EnsArgs args(opfc_ensemble *e, const int *prefix) {
   a.prefix = prefix;
   a.work = e->work;
   a.psi_hat = e->psi_hat;
-  a.tab_a = e->tab_a;
-  a.tab_b = e->tab_b;
+  a.dt = e->dt;
   a.tw = e->tw;
   a.flag = e->flag;
   return a;
 }
 
-template <typename Real, int W>
-int launch_stage_w(opfc_ensemble *e, int stage, int G) {
+// stage kernels: ensemble_f32.cu / ensemble_f64.cu
+int launch_stage(opfc_ensemble *e, int stage, int variant) {
+  const int W = var_w(variant), G = var_g(variant);
   const int wi = W == 16 ? 0 : 1;
   const int *const *pre = wi == 0 ? e->d_prefix : e->d_prefix8;
-  cudaStream_t s = e->stream;
-  if (stage == 0 || stage == 2 || stage == 3) {
-    const int axis = stage == 3 ? 2 : 1;
-    const int *p = pre[axis - 1];
-    const int tiles = e->total[wi][axis - 1];
-    const int grid = std::min(tiles, e->num_sms * G);
-    const size_t sm = ens_col_smem<Real, W>();
-    if (stage == 0)
-      ens_col_kernel<Real, W, COL_PLAIN, +1><<<grid, W * kEnsT, sm, s>>>(args(e, p), 1);
-    else if (stage == 2)
-      ens_col_kernel<Real, W, COL_PLAIN, -1><<<grid, W * kEnsT, sm, s>>>(args(e, p), 1);
-    else
-      ens_col_kernel<Real, W, COL_UPDATE, -1><<<grid, W * kEnsT, sm, s>>>(args(e, p), 2);
-  } else if (stage == 1) {
-    const int grid = std::min(e->total[wi][2], e->num_sms * G);
-    ens_x_kernel<Real, W><<<grid, W * kEnsT, ens_x_smem<Real, W>(), s>>>(args(e, pre[2]));
-  } else {
-    dim3 grid(8, e->count);
-    ens_herm_kernel<Real><<<grid, 256, 0, s>>>(args(e, nullptr));
-  }
-  return (int)cudaGetLastError();
-}
-
-template <typename Real> int launch_stage_t(opfc_ensemble *e, int stage, int variant) {
-  return var_w(variant) == 16 ? launch_stage_w<Real, 16>(e, stage, var_g(variant))
-                              : launch_stage_w<Real, 8>(e, stage, var_g(variant));
-}
-
-int launch_stage(opfc_ensemble *e, int stage, int variant) {
-  return e->prec == OPFC_FP64 ? launch_stage_t<double>(e, stage, variant)
-                              : launch_stage_t<float>(e, stage, variant);
+  // prefix sums per stage: y columns (YI, YF), z columns (ZU), x rows (X)
+  const int which = stage == 1 ? 2 : (stage == 3 ? 1 : 0);
+  const int *p = stage == 4 ? nullptr : pre[which];
+  const int tiles = stage == 4 ? 0 : e->total[wi][which];
+  const EnsArgs a = args(e, p);
+  return e->prec == OPFC_FP64 ? ens_launch_stage<double>(stage, W, G, e->num_sms, tiles, e->count, a, e->stream)
+                              : ens_launch_stage<float>(stage, W, G, e->num_sms, tiles, e->count, a, e->stream);
 }
 
 int enqueue_step(opfc_ensemble *e) {
-  const int v[5] = {e->var_col, e->var_x, e->var_col, e->var_col, 0};
+  const int v[5] = {e->var_col, e->var_x, e->var_col, e->var_upd, 0};
   for (int s = 0; s < 5; ++s) {
     const int rc = launch_stage(e, s, v[s]);
     if (rc) return efail(e, OPFC_ERR_CUDA, "ensemble stage %d: %s", s, cudaGetErrorString((cudaError_t)rc));
@@ -255,7 +231,7 @@ int opfc_ensemble_destroy(opfc_ensemble *e) {
   cudaSetDevice(e->device);
   if (e->stream) cudaStreamSynchronize(e->stream);
   drop_graph(e);
-  void *bufs[] = {e->psi_hat, e->work, e->tab_a, e->tab_b, e->tw, e->real_buf, e->d_inst, e->flag,
+  void *bufs[] = {e->psi_hat, e->work, e->tw, e->real_buf, e->d_inst, e->flag,
                   e->d_prefix[0], e->d_prefix[1], e->d_prefix[2], e->d_prefix8[0], e->d_prefix8[1],
                   e->d_prefix8[2]};
   for (void *p : bufs)
@@ -314,6 +290,8 @@ int opfc_ensemble_create(int count, const opfc_desc *descs, opfc_ensemble **out)
     in.tw1 = tw_off(in.n1);
     in.tw2 = tw_off(in.n2);
     in.mean = 0;
+    for (int a = 0; a < 3; ++a) in.kf[a] = 2.0 * 3.14159265358979323846 / (descs[i].dx[a] * descs[i].n[a]);
+    in.r = descs[i].r;
     off += (size_t)(in.M + 1) * in.n1 * in.n2;
     e->nr_max = std::max(e->nr_max, (size_t)in.n0 * in.n1 * in.n2);
   }
@@ -329,7 +307,6 @@ int opfc_ensemble_create(int count, const opfc_desc *descs, opfc_ensemble **out)
   int rc;
   const size_t cb = off * 2 * e->rsz;
   if ((rc = ealloc(ep, &ep->psi_hat, cb)) || (rc = ealloc(ep, &ep->work, cb)) ||
-      (rc = ealloc(ep, &ep->tab_a, off * e->rsz)) || (rc = ealloc(ep, &ep->tab_b, off * e->rsz)) ||
       (rc = ealloc(ep, &ep->real_buf, e->nr_max * e->rsz)) ||
       (rc = ealloc(ep, (void **)&ep->d_inst, sizeof(EnsInst) * count)) ||
       (rc = ealloc(ep, (void **)&ep->flag, sizeof(unsigned))))
@@ -372,6 +349,7 @@ int opfc_ensemble_create(int count, const opfc_desc *descs, opfc_ensemble **out)
   // dynamic shared memory above 48 KB is never needed (N <= 128)
   ep->var_col = AutoTuner::instance().get_config(ep->key + "/col", 0);
   ep->var_x = AutoTuner::instance().get_config(ep->key + "/x", 0);
+  ep->var_upd = AutoTuner::instance().get_config(ep->key + "/upd", 0);
   *out = e.release();
   return OPFC_OK;
 }
@@ -379,44 +357,9 @@ int opfc_ensemble_create(int count, const opfc_desc *descs, opfc_ensemble **out)
 int opfc_ensemble_initialize(opfc_ensemble *e, double dt) {
   if (!e) return OPFC_ERR_ARG;
   if (!(dt > 0)) return efail(e, OPFC_ERR_ARG, "dt must be positive");
-  ECUDA(e, cudaSetDevice(e->device));
-  std::vector<double> ta(e->nc_total), tb(e->nc_total);
-  const double pi = 3.14159265358979323846264338327950288;
-  auto kc = [](int i, int n, double f) { return (i <= n / 2) ? i * f : (i - n) * f; };
-  // FP64 tables per instance (10_complete_pfc_model.cpp:189-207), split layout
-  std::vector<std::thread> th;
-  const int nt = std::max(1, std::min(e->count, (int)std::thread::hardware_concurrency()));
-  for (int w = 0; w < nt; ++w)
-    th.emplace_back([&, w] {
-      for (int i = w; i < e->count; i += nt) {
-        const EnsInst &in = e->inst[i];
-        const opfc_desc &d = e->desc[i];
-        const double f0 = 2.0 * pi / (d.dx[0] * in.n0), f1 = 2.0 * pi / (d.dx[1] * in.n1),
-                     f2 = 2.0 * pi / (d.dx[2] * in.n2);
-        for (int kz = 0; kz < in.n2; ++kz)
-          for (int ky = 0; ky < in.n1; ++ky)
-            for (int kx = 0; kx <= in.M; ++kx) {
-              const double a = kc(kx, in.n0, f0), b = kc(ky, in.n1, f1), c = kc(kz, in.n2, f2);
-              const double k2 = a * a + b * b + c * c, k2l = -k2;
-              const double L = k2l * (d.r + (1.0 - k2) * (1.0 - k2));
-              const double eL = std::exp(L * dt);
-              const size_t row = (size_t)ky + (size_t)in.n1 * kz;
-              const size_t o = in.off_c + (kx < in.M ? kx + (size_t)in.M * row
-                                                       : (size_t)in.M * in.n1 * in.n2 + row);
-              ta[o] = eL;
-              tb[o] = (std::fabs(L) > 1e-14) ? (eL - 1.0) / L * k2l : dt * k2l;
-            }
-      }
-    });
-  for (auto &t : th) t.join();
-  if (e->prec == OPFC_FP64) {
-    ECUDA(e, cudaMemcpy(e->tab_a, ta.data(), ta.size() * 8, cudaMemcpyHostToDevice));
-    ECUDA(e, cudaMemcpy(e->tab_b, tb.data(), tb.size() * 8, cudaMemcpyHostToDevice));
-  } else {
-    std::vector<float> fa(ta.begin(), ta.end()), fb(tb.begin(), tb.end());
-    ECUDA(e, cudaMemcpy(e->tab_a, fa.data(), fa.size() * 4, cudaMemcpyHostToDevice));
-    ECUDA(e, cudaMemcpy(e->tab_b, fb.data(), fb.size() * 4, cudaMemcpyHostToDevice));
-  }
+  // the operators of every instance are computed per mode inside the z
+  // update (10_complete_pfc_model.cpp:189-207 with opL = 1 + expm1(L dt),
+  // opN = expm1(L dt) / (r + (1 - k^2)^2)) from its r, k steps and dt
   e->dt = dt;
   e->initialized = true;
   drop_graph(e);
@@ -526,16 +469,18 @@ int opfc_ensemble_sync(opfc_ensemble *e) {
   return OPFC_OK;
 }
 
-int opfc_ensemble_autotune(opfc_ensemble *e, double *ms_col, double *ms_x) {
+int opfc_ensemble_autotune(opfc_ensemble *e, double *ms_col, double *ms_x, double *ms_upd) {
   if (!e) return OPFC_ERR_ARG;
   if (!e->initialized) return efail(e, OPFC_ERR_STATE, "initialize before tuning");
   ECUDA(e, cudaSetDevice(e->device));
-  std::vector<double> mc, mx;
+  std::vector<double> mc, mx, mu;
   // the passes run in place on whatever the arrays hold; states are re-set after
   e->var_col = AutoTuner::instance().tune(e->key + "/col", kVariants,
                                           [&](int v) { return launch_stage(e, 2, v); }, e->stream, &mc);
   e->var_x = AutoTuner::instance().tune(e->key + "/x", kVariants, [&](int v) { return launch_stage(e, 1, v); },
                                         e->stream, &mx);
+  e->var_upd = AutoTuner::instance().tune(e->key + "/upd", kVariants,
+                                          [&](int v) { return launch_stage(e, 3, v); }, e->stream, &mu);
   ECUDA(e, cudaStreamSynchronize(e->stream));
   cudaMemset(e->flag, 0, sizeof(unsigned));
   for (int i = 0; i < e->count; ++i) e->have_state[i] = false;
@@ -545,13 +490,16 @@ int opfc_ensemble_autotune(opfc_ensemble *e, double *ms_col, double *ms_x) {
     for (int v = 0; v < kVariants; ++v) ms_col[v] = mc.empty() ? -1 : mc[v];
   if (ms_x)
     for (int v = 0; v < kVariants; ++v) ms_x[v] = mx.empty() ? -1 : mx[v];
+  if (ms_upd)
+    for (int v = 0; v < kVariants; ++v) ms_upd[v] = mu.empty() ? -1 : mu[v];
   return OPFC_OK;
 }
 
-int opfc_ensemble_variants(const opfc_ensemble *e, int *var_col, int *var_x) {
-  if (!e || !var_col || !var_x) return OPFC_ERR_ARG;
+int opfc_ensemble_variants(const opfc_ensemble *e, int *var_col, int *var_x, int *var_upd) {
+  if (!e || !var_col || !var_x || !var_upd) return OPFC_ERR_ARG;
   *var_col = e->var_col;
   *var_x = e->var_x;
+  *var_upd = e->var_upd;
   return OPFC_OK;
 }
 

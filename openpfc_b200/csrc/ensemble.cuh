@@ -12,12 +12,17 @@
 
 namespace opfc {
 
+OPFC_EXTERN(float)
+OPFC_EXTERN(double)
+
 struct EnsInst {
   int n0, n1, n2, M;
   long long off_c;     // element offset of the instance's split-layout arrays
   int tw0, tw1, tw2;   // element offsets of its x (N0), y (N1), z (N2) twiddles
   int pad_;
   double mean;         // mean density (k = 0 mode, FP64)
+  double kf[3];        // wavenumber steps 2 pi / (dx_a N_a)
+  double r;            // the instance's r (operators computed per mode)
 };
 
 struct EnsArgs {
@@ -26,9 +31,9 @@ struct EnsArgs {
   const int *prefix;   // tile prefix sums of this stage, count + 1 entries
   void *work;          // F_z^-1 of the states / the step's working arrays
   void *psi_hat;       // states (DC slot zero)
-  const void *tab_a, *tab_b;
   const void *tw;      // concatenated twiddle tables
   unsigned *flag;
+  double dt;
 };
 
 constexpr int kEnsT = 4;  // threads per line
@@ -64,12 +69,15 @@ __device__ __forceinline__ void ens_col_tile(const EnsArgs &a, const EnsInst &in
   long long base;
   long long fs;
   bool ok;
+  int kx, ky;  // z pass: the column's (kx, ky)
   if (t < ti_main * n_outer) {
     const int ti = t % ti_main, to = t / ti_main;
     const int cg = ti * W + c;
     ok = cg < M;
     base = (axis == 1 ? (long long)to * M * n1 : (long long)to * M) + cg;
     fs = axis == 1 ? M : (long long)M * n1;
+    kx = cg;
+    ky = to;
   } else {
     const int tn = t - ti_main * n_outer;
     const int cg = tn * W + c;
@@ -77,6 +85,8 @@ __device__ __forceinline__ void ens_col_tile(const EnsArgs &a, const EnsInst &in
     ok = cg < ncols;
     base = nyq + (axis == 1 ? (long long)cg * n1 : (long long)cg);
     fs = axis == 1 ? 1 : n1;
+    kx = M;
+    ky = cg;
   }
   C *work = reinterpret_cast<C *>(a.work) + in.off_c;
   C v[E];
@@ -85,20 +95,45 @@ __device__ __forceinline__ void ens_col_tile(const EnsArgs &a, const EnsInst &in
   if constexpr (MODE == COL_PLAIN) {
     fft_line_e<C, N, DIR, N>(v, sm, ld, c, j, tw);
   } else {
-    fft_line_e<C, N, -1, N>(v, sm, ld, c, j, tw);
+    // z update: psi_hat <- opL psi_hat + opN N_hat with opL, opN computed from
+    // k^2 and the instance's r.  The tile's psi_hat values are loaded as one
+    // batch -- before the transform when they fit in registers beside it -- so
+    // the tile waits on memory once, not once per value.
     C *ph = reinterpret_cast<C *>(a.psi_hat) + in.off_c;
-    const Real *ta = reinterpret_cast<const Real *>(a.tab_a) + in.off_c;
-    const Real *tb = reinterpret_cast<const Real *>(a.tab_b) + in.off_c;
+    // EARLY: the whole batch fits beside v (E <= 16 values); otherwise batches
+    // of B values after the transform
+    constexpr bool EARLY = E * sizeof(C) <= 16 * 8;
+    constexpr int B = EARLY ? E : (E % 8 == 0 ? 8 : (E % 6 == 0 ? 6 : 4));
+    static_assert(E % B == 0, "update batch");
+    C p[EARLY ? E : B];
+    if constexpr (EARLY) {
 #pragma unroll
-    for (int m = 0; m < E; ++m) {
-      const long long idx = base + (long long)(j + kEnsT * m) * fs;
-      C np = mk<C>(0, 0);
-      if (ok) {
-        const C p = ph[idx];
-        np = mk<C>(ta[idx] * p.x + tb[idx] * v[m].x, ta[idx] * p.y + tb[idx] * v[m].y);
-        ph[idx] = np;
+      for (int m = 0; m < E; ++m) p[m] = ok ? ph[base + (long long)(j + kEnsT * m) * fs] : mk<C>(0, 0);
+    }
+    fft_line_e<C, N, -1, N>(v, sm, ld, c, j, tw);
+    const int fy = ky <= n1 / 2 ? ky : n1 - ky;
+    const Real qx = Real(in.kf[0]) * Real(kx), qy = Real(in.kf[1]) * Real(fy);
+    const Real qxy = qx * qx + qy * qy;
+    const Real kf2 = Real(in.kf[2]), r = Real(in.r), dt = Real(a.dt);
+#pragma unroll
+    for (int m0 = 0; m0 < E; m0 += B) {
+      if constexpr (!EARLY) {
+#pragma unroll
+        for (int q = 0; q < B; ++q)
+          p[q] = ok ? ph[base + (long long)(j + kEnsT * (m0 + q)) * fs] : mk<C>(0, 0);
       }
-      v[m] = np;
+#pragma unroll
+      for (int q = 0; q < B; ++q) {
+        const int m = m0 + q;
+        const int kz = j + kEnsT * m;
+        const int fz = kz <= n2 / 2 ? kz : n2 - kz;
+        const Real qz = kf2 * Real(fz);
+        Real la, lb;
+        ops_from_k2(qxy + qz * qz, r, dt, la, lb);
+        const C pm = p[EARLY ? m : q];
+        v[m] = mk<C>(la * pm.x + lb * v[m].x, la * pm.y + lb * v[m].y);
+        if (ok) ph[base + (long long)kz * fs] = v[m];
+      }
     }
     fft_line_e<C, N, +1, N>(v, sm, ld, c, j, tw);
   }
@@ -109,8 +144,13 @@ __device__ __forceinline__ void ens_col_tile(const EnsArgs &a, const EnsInst &in
   __syncthreads();  // tw / sm are reused by the next tile
 }
 
-template <typename Real, int W, int MODE, int DIR>
-__global__ void __launch_bounds__(W *kEnsT) ens_col_kernel(const EnsArgs a, int axis) {
+// G = CTAs per SM the kernel is compiled for (__launch_bounds__ minimum): one
+// kernel serves every length, so its register budget would otherwise be set
+// by the longest line (32 values per thread at N = 128); a larger G caps the
+// registers (65536 / (G * threads)) and trades spills in the long branches for
+// occupancy in the short ones.  The autotuner times every (W, G).
+template <typename Real, int W, int MODE, int DIR, int G>
+__global__ void __launch_bounds__(W *kEnsT, G) ens_col_kernel(const EnsArgs a, int axis) {
   using C = typename Cx<Real>::T;
   extern __shared__ __align__(16) unsigned char smraw[];
   C *tw = reinterpret_cast<C *>(smraw);
@@ -157,11 +197,12 @@ __device__ __forceinline__ void ens_x_tile(const EnsArgs &a, const EnsInst &in, 
   x_pre<C, M, W, E>(buf, tw, c, j, v);
   __syncthreads();
   fft_line_e<C, M, +1, N0>(v, buf, ld, c, j, tw);
-  const double scale = 1.0 / ((double)in.n0 * rows);
+  // normalisation and mean in the compute precision (as the single-grid x pass)
+  const Real sc = Real(1.0 / ((double)in.n0 * rows)), mn = Real(in.mean);
 #pragma unroll
   for (int m = 0; m < E; ++m) {
-    const Real x = to_real_plus_mean(v[m].x, scale, in.mean);
-    const Real y = to_real_plus_mean(v[m].y, scale, in.mean);
+    const Real x = v[m].x * sc + mn;
+    const Real y = v[m].y * sc + mn;
     const Real nx = x * x * x, ny = y * y * y;
     bad |= !(isfinite(nx) && isfinite(ny));
     v[m] = mk<C>(nx, ny);
@@ -174,8 +215,8 @@ __device__ __forceinline__ void ens_x_tile(const EnsArgs &a, const EnsInst &in, 
   __syncthreads();
 }
 
-template <typename Real, int W>
-__global__ void __launch_bounds__(W *kEnsT) ens_x_kernel(const EnsArgs a) {
+template <typename Real, int W, int G>
+__global__ void __launch_bounds__(W *kEnsT, G) ens_x_kernel(const EnsArgs a) {
   using C = typename Cx<Real>::T;
   extern __shared__ __align__(16) unsigned char smraw[];
   C *tw = reinterpret_cast<C *>(smraw);
@@ -234,5 +275,42 @@ template <typename Real, int W> constexpr size_t ens_col_smem() {
 template <typename Real, int W> constexpr size_t ens_x_smem() {
   return sizeof(typename Cx<Real>::T) * (128 + 65 * (W + 1));
 }
+
+template <typename Real, int W, int G>
+int ens_launch_stage_w(int stage, int num_sms, int tiles, int count, const EnsArgs &a, cudaStream_t s) {
+  const int grid = tiles < num_sms * G ? tiles : num_sms * G;
+  if (stage == 0 || stage == 2 || stage == 3) {
+    const size_t sm = ens_col_smem<Real, W>();
+    if (stage == 0)
+      ens_col_kernel<Real, W, COL_PLAIN, +1, G><<<grid, W * kEnsT, sm, s>>>(a, 1);
+    else if (stage == 2)
+      ens_col_kernel<Real, W, COL_PLAIN, -1, G><<<grid, W * kEnsT, sm, s>>>(a, 1);
+    else
+      ens_col_kernel<Real, W, COL_UPDATE, -1, G><<<grid, W * kEnsT, sm, s>>>(a, 2);
+  } else if (stage == 1) {
+    ens_x_kernel<Real, W, G><<<grid, W * kEnsT, ens_x_smem<Real, W>(), s>>>(a);
+  } else {
+    ens_herm_kernel<Real><<<dim3(8, count), 256, 0, s>>>(a);
+  }
+  return (int)cudaGetLastError();
+}
+
+// One stage of the ensemble step (0 y inverse, 1 fused x, 2 y forward, 3 z
+// update, 4 Hermitian fix) with tiles of W = 16 or 8 lines and at most G CTAs
+// per SM; `tiles` is the stage's tile count (a.prefix[count]).  Instantiated
+// per precision in ensemble_f32.cu / ensemble_f64.cu.
+template <typename Real>
+int ens_launch_stage(int stage, int W, int G, int num_sms, int tiles, int count, const EnsArgs &a,
+                     cudaStream_t s) {
+#define OPFC_ENS_WG(w, g) \
+  if (W == w && G == g) return ens_launch_stage_w<Real, w, g>(stage, num_sms, tiles, count, a, s);
+  OPFC_ENS_WG(16, 4) OPFC_ENS_WG(16, 8) OPFC_ENS_WG(16, 16)
+  OPFC_ENS_WG(8, 4) OPFC_ENS_WG(8, 8) OPFC_ENS_WG(8, 16)
+#undef OPFC_ENS_WG
+  return (int)cudaErrorInvalidValue;
+}
+
+extern template int ens_launch_stage<float>(int, int, int, int, int, int, const EnsArgs &, cudaStream_t);
+extern template int ens_launch_stage<double>(int, int, int, int, int, int, const EnsArgs &, cudaStream_t);
 
 }  // namespace opfc

@@ -55,6 +55,16 @@ enum OpsKind { OPS_TABLES = 0, OPS_RADIAL = 1, OPS_COMPUTED = 2 };
 __device__ __forceinline__ float ops_div(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ double ops_div(double a, double b) { return a / b; }
 
+template <typename Real>
+__device__ __forceinline__ void ops_from_k2(Real k2, Real r, Real dt, Real &la, Real &lb) {
+  const Real u = Real(1) - k2;
+  const Real g = r + u * u;
+  const Real L = -k2 * g;
+  const Real em1 = expm1(L * dt);
+  la = Real(1) + em1;
+  lb = fabs(L) > Real(1e-14) ? ops_div(em1, g) : -dt * k2;
+}
+
 template <typename Real, int MODEL>
 __device__ __forceinline__ void computed_ops(const ColArgs<Real> &a, int kx, int ky, int kz, Real &la,
                                              Real &lb, Real &ch) {
@@ -62,12 +72,7 @@ __device__ __forceinline__ void computed_ops(const ColArgs<Real> &a, int kx, int
   const int fz = kz <= a.rad_n2 / 2 ? kz : a.rad_n2 - kz;
   const Real qx = a.kf0 * Real(kx), qy = a.kf1 * Real(fy), qz = a.kf2 * Real(fz);
   const Real k2 = qx * qx + qy * qy + qz * qz;
-  const Real u = Real(1) - k2;
-  const Real g = a.op_r + u * u;
-  const Real L = -k2 * g;
-  const Real em1 = expm1(L * a.op_dt);
-  la = Real(1) + em1;
-  lb = fabs(L) > Real(1e-14) ? ops_div(em1, g) : -a.op_dt * k2;
+  ops_from_k2(k2, a.op_r, a.op_dt, la, lb);
   ch = MODEL == MK_FILTERED ? exp(-k2 * a.op_chi) : Real(1);
 }
 
@@ -1060,5 +1065,20 @@ int launch_energy_k(const void *psi_hat, int M, int n1, int n2, long long nyq_of
   template int launch_sum_pow<R>(const void *, size_t, int, double *, int, cudaStream_t);            \
   template int launch_energy_k<R>(const void *, int, int, int, long long, const double *, double,    \
                                   double *, int, cudaStream_t);
+
+// Other translation units that include this header (ensemble*.cu) call the
+// launchers without instantiating the pass kernels a second time; the
+// instantiations live in kernels_f32.cu and kernels_f64.cu.
+#define OPFC_EXTERN(R)                                                                                      \
+  extern template int launch_col<R>(const ColLaunch &, cudaStream_t);                                       \
+  extern template int launch_x<R>(const XLaunch &, cudaStream_t);                                           \
+  extern template int launch_herm_fix<R>(void *, long long, int, int, int, cudaStream_t, double *, double);  \
+  extern template int launch_to_ref<R>(const void *, void *, int, int, int, int, long long, int, double,    \
+                                       cudaStream_t);                                                       \
+  extern template int launch_from_ref<R>(const void *, int, void *, int, int, int, long long, cudaStream_t); \
+  extern template int launch_cast_real<R>(const void *, int, void *, int, size_t, cudaStream_t);            \
+  extern template int launch_sum_pow<R>(const void *, size_t, int, double *, int, cudaStream_t);            \
+  extern template int launch_energy_k<R>(const void *, int, int, int, long long, const double *, double,    \
+                                         double *, int, cudaStream_t);
 
 }  // namespace opfc

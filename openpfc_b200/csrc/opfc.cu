@@ -379,7 +379,8 @@ double mean_density(const opfc_handle *h) { return h->mass_sum / (double)h->nr; 
 
 // autotuner cache key of one pass of this handle's step
 std::string tune_key(const opfc_handle *h, const char *pass) {
-  static const char *models[] = {"plain", "tungsten", "filtered", "aluminum"};
+  static const char *models[] = {"plain", "tungsten", "filtered", "aluminum", "user_etd"};
+  static_assert(sizeof(models) / sizeof(models[0]) == OPFC_MODEL_USER_ETD + 1, "a name per model");
   char b[160];
   std::snprintf(b, sizeof b, "step/%s/%s/%dx%dx%d/%s/f%s", h->prec == OPFC_FP64 ? "fp64" : "fp32",
                 models[h->desc.model], h->n0, h->n1, h->n2, pass,

@@ -54,8 +54,9 @@ def test_ensemble_autotune_keeps_results(oracle, tmp_path, monkeypatch):
     ms = members(6, 9)
     e = ob.Ensemble(ms, precision=ob.FP32)
     e.initialize(0.5)
-    mc, mx = e.autotune()
-    assert min(v for v in mc if v > 0) > 0 and min(v for v in mx if v > 0) > 0
+    mc, mx, mu = e.autotune()
+    assert all(min(v for v in ms if v > 0) > 0 for ms in (mc, mx, mu))
+    assert all(0 <= v < 6 for v in e.variants())
     psi0 = [ob.ic_noise(m["n"], m["n0"], 0.01, m["seed"]) for m in ms]
     for i, p in enumerate(psi0):
         e.set_psi(i, p)
