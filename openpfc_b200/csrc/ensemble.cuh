@@ -50,10 +50,25 @@ __device__ __forceinline__ int ens_find(const int *prefix, int count, int g) {
   return lo;
 }
 
+// Per-thread asynchronous copy of one complex value from global to shared
+// memory (cp.async, 8 or 16 bytes); cp_async_wait_all() waits for this
+// thread's copies only.
+template <typename C> __device__ __forceinline__ void cp_async_value(C *dst, const C *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  const size_t g = __cvta_generic_to_global(src);
+  if constexpr (sizeof(C) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(g) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 // Column tile (y or z pass) of one instance; mirrors col_kernel's body.
+// pbuf (z update only): N x W complex staging space for the tile's psi_hat.
 template <typename Real, int N, int W, int MODE, int DIR>
 __device__ __forceinline__ void ens_col_tile(const EnsArgs &a, const EnsInst &in, int axis, int t,
-                                             typename Cx<Real>::T *tw, typename Cx<Real>::T *sm) {
+                                             typename Cx<Real>::T *tw, typename Cx<Real>::T *sm,
+                                             typename Cx<Real>::T *pbuf) {
   using C = typename Cx<Real>::T;
   constexpr int E = N / kEnsT;
   constexpr int ld = W + 1;
@@ -100,40 +115,29 @@ __device__ __forceinline__ void ens_col_tile(const EnsArgs &a, const EnsInst &in
     // batch -- before the transform when they fit in registers beside it -- so
     // the tile waits on memory once, not once per value.
     C *ph = reinterpret_cast<C *>(a.psi_hat) + in.off_c;
-    // EARLY: the whole batch fits beside v (E <= 16 values); otherwise batches
-    // of B values after the transform
-    constexpr bool EARLY = E * sizeof(C) <= 16 * 8;
-    constexpr int B = EARLY ? E : (E % 8 == 0 ? 8 : (E % 6 == 0 ? 6 : 4));
-    static_assert(E % B == 0, "update batch");
-    C p[EARLY ? E : B];
-    if constexpr (EARLY) {
+    // the tile's psi_hat is copied to shared memory while the forward
+    // transform runs; each thread reads back only the values it copied
+    if (ok) {
 #pragma unroll
-      for (int m = 0; m < E; ++m) p[m] = ok ? ph[base + (long long)(j + kEnsT * m) * fs] : mk<C>(0, 0);
+      for (int m = 0; m < E; ++m)
+        cp_async_value(pbuf + (j + kEnsT * m) * W + c, ph + base + (long long)(j + kEnsT * m) * fs);
     }
     fft_line_e<C, N, -1, N>(v, sm, ld, c, j, tw);
+    cp_async_wait_all();
     const int fy = ky <= n1 / 2 ? ky : n1 - ky;
     const Real qx = Real(in.kf[0]) * Real(kx), qy = Real(in.kf[1]) * Real(fy);
     const Real qxy = qx * qx + qy * qy;
     const Real kf2 = Real(in.kf[2]), r = Real(in.r), dt = Real(a.dt);
 #pragma unroll
-    for (int m0 = 0; m0 < E; m0 += B) {
-      if constexpr (!EARLY) {
-#pragma unroll
-        for (int q = 0; q < B; ++q)
-          p[q] = ok ? ph[base + (long long)(j + kEnsT * (m0 + q)) * fs] : mk<C>(0, 0);
-      }
-#pragma unroll
-      for (int q = 0; q < B; ++q) {
-        const int m = m0 + q;
-        const int kz = j + kEnsT * m;
-        const int fz = kz <= n2 / 2 ? kz : n2 - kz;
-        const Real qz = kf2 * Real(fz);
-        Real la, lb;
-        ops_from_k2(qxy + qz * qz, r, dt, la, lb);
-        const C pm = p[EARLY ? m : q];
-        v[m] = mk<C>(la * pm.x + lb * v[m].x, la * pm.y + lb * v[m].y);
-        if (ok) ph[base + (long long)kz * fs] = v[m];
-      }
+    for (int m = 0; m < E; ++m) {
+      const int kz = j + kEnsT * m;
+      const int fz = kz <= n2 / 2 ? kz : n2 - kz;
+      const Real qz = kf2 * Real(fz);
+      Real la, lb;
+      ops_from_k2(qxy + qz * qz, r, dt, la, lb);
+      const C pm = ok ? pbuf[kz * W + c] : mk<C>(0, 0);
+      v[m] = mk<C>(la * pm.x + lb * v[m].x, la * pm.y + lb * v[m].y);
+      if (ok) ph[base + (long long)kz * fs] = v[m];
     }
     fft_line_e<C, N, +1, N>(v, sm, ld, c, j, tw);
   }
@@ -155,6 +159,7 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_col_kernel(const EnsArgs a, i
   extern __shared__ __align__(16) unsigned char smraw[];
   C *tw = reinterpret_cast<C *>(smraw);
   C *sm = tw + 128;
+  C *pb = sm + 128 * (W + 1);  // z update: psi_hat staging (ens_col_smem)
   const int total = a.prefix[a.count];
   for (int g = blockIdx.x; g < total; g += gridDim.x) {
     const int i = ens_find(a.prefix, a.count, g);
@@ -162,13 +167,13 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_col_kernel(const EnsArgs a, i
     const int t = g - a.prefix[i];
     const int N = axis == 1 ? in.n1 : in.n2;
     switch (N) {
-      case 16: ens_col_tile<Real, 16, W, MODE, DIR>(a, in, axis, t, tw, sm); break;
-      case 32: ens_col_tile<Real, 32, W, MODE, DIR>(a, in, axis, t, tw, sm); break;
-      case 48: ens_col_tile<Real, 48, W, MODE, DIR>(a, in, axis, t, tw, sm); break;
-      case 64: ens_col_tile<Real, 64, W, MODE, DIR>(a, in, axis, t, tw, sm); break;
-      case 80: ens_col_tile<Real, 80, W, MODE, DIR>(a, in, axis, t, tw, sm); break;
-      case 96: ens_col_tile<Real, 96, W, MODE, DIR>(a, in, axis, t, tw, sm); break;
-      case 128: ens_col_tile<Real, 128, W, MODE, DIR>(a, in, axis, t, tw, sm); break;
+      case 16: ens_col_tile<Real, 16, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
+      case 32: ens_col_tile<Real, 32, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
+      case 48: ens_col_tile<Real, 48, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
+      case 64: ens_col_tile<Real, 64, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
+      case 80: ens_col_tile<Real, 80, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
+      case 96: ens_col_tile<Real, 96, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
+      case 128: ens_col_tile<Real, 128, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
       default: break;  // sizes are validated on the host
     }
   }
@@ -269,26 +274,47 @@ __global__ void ens_herm_kernel(const EnsArgs a) {
 }
 
 // largest dynamic shared memory any ensemble kernel needs (N, M <= 128 / 64)
-template <typename Real, int W> constexpr size_t ens_col_smem() {
-  return sizeof(typename Cx<Real>::T) * (128 + 128 * (W + 1));
+template <typename Real, int W, int MODE = COL_PLAIN> constexpr size_t ens_col_smem() {
+  return sizeof(typename Cx<Real>::T) * (128 + 128 * (W + 1) + (MODE == COL_UPDATE ? 128 * W : 0));
 }
 template <typename Real, int W> constexpr size_t ens_x_smem() {
   return sizeof(typename Cx<Real>::T) * (128 + 65 * (W + 1));
 }
 
+// Persistent launch of kernel k: G CTAs per SM, or as many as fit (a CTA that
+// is not resident would hold its whole tile list back until a slot frees).
+template <typename K, typename... Args>
+int ens_persistent(K k, int G, int num_sms, int tiles, size_t smem, int threads, cudaStream_t s, int &occ,
+                   const Args &...args) {
+  if (!occ) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess || occ < 1) occ = 1;
+    if (occ > G) occ = G;
+  }
+  const int grid = tiles < num_sms * occ ? tiles : num_sms * occ;
+  if (grid < 1) return 0;
+  k<<<grid, threads, smem, s>>>(args...);
+  return (int)cudaGetLastError();
+}
+
 template <typename Real, int W, int G>
 int ens_launch_stage_w(int stage, int num_sms, int tiles, int count, const EnsArgs &a, cudaStream_t s) {
-  const int grid = tiles < num_sms * G ? tiles : num_sms * G;
-  if (stage == 0 || stage == 2 || stage == 3) {
-    const size_t sm = ens_col_smem<Real, W>();
-    if (stage == 0)
-      ens_col_kernel<Real, W, COL_PLAIN, +1, G><<<grid, W * kEnsT, sm, s>>>(a, 1);
-    else if (stage == 2)
-      ens_col_kernel<Real, W, COL_PLAIN, -1, G><<<grid, W * kEnsT, sm, s>>>(a, 1);
-    else
-      ens_col_kernel<Real, W, COL_UPDATE, -1, G><<<grid, W * kEnsT, sm, s>>>(a, 2);
+  constexpr int NT = W * kEnsT;
+  if (stage == 0) {
+    static int occ = 0;
+    return ens_persistent(ens_col_kernel<Real, W, COL_PLAIN, +1, G>, G, num_sms, tiles, ens_col_smem<Real, W>(),
+                          NT, s, occ, a, 1);
+  } else if (stage == 2) {
+    static int occ = 0;
+    return ens_persistent(ens_col_kernel<Real, W, COL_PLAIN, -1, G>, G, num_sms, tiles, ens_col_smem<Real, W>(),
+                          NT, s, occ, a, 1);
+  } else if (stage == 3) {
+    static int occ = 0;
+    return ens_persistent(ens_col_kernel<Real, W, COL_UPDATE, -1, G>, G, num_sms, tiles,
+                          ens_col_smem<Real, W, COL_UPDATE>(), NT, s, occ, a, 2);
   } else if (stage == 1) {
-    ens_x_kernel<Real, W, G><<<grid, W * kEnsT, ens_x_smem<Real, W>(), s>>>(a);
+    static int occ = 0;
+    return ens_persistent(ens_x_kernel<Real, W, G>, G, num_sms, tiles, ens_x_smem<Real, W>(), NT, s, occ, a);
   } else {
     ens_herm_kernel<Real><<<dim3(8, count), 256, 0, s>>>(a);
   }
