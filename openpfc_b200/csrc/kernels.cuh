@@ -136,30 +136,45 @@ __global__ void __launch_bounds__(Width<Real>::W *(N / EE)) col_kernel(const Col
     C *ph = reinterpret_cast<C *>(a.psi_hat);
     C w[(MODEL == MK_PLAIN) ? 1 : E];
     C pw[(MODEL == MK_ALUMINUM_G) ? E : 1];
+    // psi_hat in groups of GB values: each group's loads are issued together,
+    // then combined and stored (a store to psi_hat keeps every later load --
+    // psi_hat, tables -- behind it, so a value-by-value loop would make one
+    // memory round trip per value; larger groups cost registers)
+    constexpr int GB = E % 4 == 0 ? 4 : 1;
 #pragma unroll
-    for (int m = 0; m < E; ++m) {
-      const long long idx = base + (long long)(j + T * m) * fs;
-      C np = czero<C>();
-      if constexpr (MODEL == MK_ALUMINUM_G) pw[m] = czero<C>();
-      if (ok) {
-        const C p = ph[idx];
-        Real la, lb, ch = Real(1);
-        if constexpr (OPS == OPS_COMPUTED) {
-          // z pass: main plane kx = column, ky = outer; Nyquist plane kx = M, ky = column
-          computed_ops<Real, MODEL>(a, second ? a.rad_M : cg, second ? cg : to, j + T * m, la, lb, ch);
-        } else {
-          la = a.tab_a[idx];
-          lb = a.tab_b[idx];
-          if constexpr (MODEL != MK_PLAIN) ch = a.tab_chi[idx];
+    for (int m0 = 0; m0 < E; m0 += GB) {
+      C pv[GB];
+#pragma unroll
+      for (int q = 0; q < GB; ++q) pv[q] = ok ? ph[base + (long long)(j + T * (m0 + q)) * fs] : czero<C>();
+#pragma unroll
+      for (int q = 0; q < GB; ++q) {
+        const int m = m0 + q;
+        const long long idx = base + (long long)(j + T * m) * fs;
+        C np = czero<C>();
+        if constexpr (MODEL == MK_ALUMINUM_G) pw[m] = czero<C>();
+        if (ok) {
+          const C p = pv[q];
+          Real la, lb, ch = Real(1);
+          if constexpr (OPS == OPS_COMPUTED) {
+            // z pass: main plane kx = column, ky = outer; Nyquist plane kx = M, ky = column
+            computed_ops<Real, MODEL>(a, second ? a.rad_M : cg, second ? cg : to, j + T * m, la, lb, ch);
+          } else {
+            la = a.tab_a[idx];
+            lb = a.tab_b[idx];
+            if constexpr (MODEL != MK_PLAIN) ch = a.tab_chi[idx];
+          }
+          np = mk<C>(la * p.x + lb * v[m].x, la * p.y + lb * v[m].y);
+          if constexpr (MODEL != MK_PLAIN) w[m] = cscale(np, ch);
+          if constexpr (MODEL == MK_ALUMINUM_G) pw[m] = cscale(np, a.tab_p[idx]);
+        } else if constexpr (MODEL != MK_PLAIN) {
+          w[m] = czero<C>();
         }
-        np = mk<C>(la * p.x + lb * v[m].x, la * p.y + lb * v[m].y);
-        ph[idx] = np;
-        if constexpr (MODEL != MK_PLAIN) w[m] = cscale(np, ch);
-        if constexpr (MODEL == MK_ALUMINUM_G) pw[m] = cscale(np, a.tab_p[idx]);
-      } else if constexpr (MODEL != MK_PLAIN) {
-        w[m] = czero<C>();
+        v[m] = np;
       }
-      v[m] = np;
+      if (ok) {
+#pragma unroll
+        for (int q = 0; q < GB; ++q) ph[base + (long long)(j + T * (m0 + q)) * fs] = v[m0 + q];
+      }
     }
     if constexpr (INV) {
       if constexpr (MODEL == MK_FILTERED) {
