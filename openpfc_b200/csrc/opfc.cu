@@ -1212,8 +1212,16 @@ int opfc_set_psi(opfc_handle *h, const void *psi, size_t count, int dtype, int w
   CUDA_TRY(h, cudaSetDevice(h->device));
   if ((rc = real_in(h, psi, dtype, where))) return rc;
   // k = 0 mode in FP64 with compensated summation of the caller's values in
-  // their own precision (before any rounding to the compute precision)
-  if ((rc = user_sum(h, psi, dtype, where, &h->mass_sum))) return rc;
+  // their own precision (before any rounding to the compute precision).  A
+  // host field already in the compute precision arrives bit for bit in the
+  // device buffer, so its sum runs there (one pass of the GPU) instead of on
+  // the host threads after the copy.
+  const bool same_prec = (dtype == OPFC_F64) == (h->prec == OPFC_FP64);
+  if (where == OPFC_HOST && same_prec)
+    rc = user_sum(h, h->real_buf, dtype, OPFC_DEVICE, &h->mass_sum);
+  else
+    rc = user_sum(h, psi, dtype, where, &h->mass_sum);
+  if (rc) return rc;
   if ((rc = forward_real_buf(h, h->psi_hat))) return rc;
   // the DC slot of the FP32/FP64 array stays zero; mass_sum carries it
   CUDA_TRY(h, cudaMemsetAsync(h->psi_hat, 0, 2 * h->rsz, h->stream));
