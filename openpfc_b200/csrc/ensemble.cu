@@ -51,6 +51,12 @@ struct opfc_ensemble {
   int *d_prefix[3] = {nullptr, nullptr, nullptr};  // y col, z col, x tiles (per W variant)
   int total[2][3] = {};                           // [W = 16, 8][stage]
   int *d_prefix8[3] = {nullptr, nullptr, nullptr};
+  // members per stage kind (y columns, z columns, x rows) sorted by that
+  // stage's line length, longest first: CTAs that run at the same time then
+  // run the same length's code (one kernel holds every length's unrolled
+  // transforms; mixing them thrashed the instruction cache) and the longest
+  // tiles start first
+  int *d_order[3] = {nullptr, nullptr, nullptr};
   unsigned *flag = nullptr;
   int var_col = 0, var_x = 0, var_upd = 0;  // y passes, x pass, z update
   cudaGraphExec_t graph = nullptr;
@@ -93,11 +99,12 @@ int col_tiles(const EnsInst &in, int axis, int W) {
 }
 int x_tiles(const EnsInst &in, int W) { return (in.n1 * in.n2 + W - 1) / W; }
 
-EnsArgs args(opfc_ensemble *e, const int *prefix) {
+EnsArgs args(opfc_ensemble *e, const int *prefix, const int *order) {
   EnsArgs a;
   a.inst = e->d_inst;
   a.count = e->count;
   a.prefix = prefix;
+  a.order = order;
   a.work = e->work;
   a.psi_hat = e->psi_hat;
   a.dt = e->dt;
@@ -115,7 +122,7 @@ int launch_stage(opfc_ensemble *e, int stage, int variant) {
   const int which = stage == 1 ? 2 : (stage == 3 ? 1 : 0);
   const int *p = stage == 4 ? nullptr : pre[which];
   const int tiles = stage == 4 ? 0 : e->total[wi][which];
-  const EnsArgs a = args(e, p);
+  const EnsArgs a = args(e, p, stage == 4 ? nullptr : e->d_order[which]);
   return e->prec == OPFC_FP64 ? ens_launch_stage<double>(stage, W, G, e->num_sms, tiles, e->count, a, e->stream)
                               : ens_launch_stage<float>(stage, W, G, e->num_sms, tiles, e->count, a, e->stream);
 }
@@ -233,7 +240,7 @@ int opfc_ensemble_destroy(opfc_ensemble *e) {
   drop_graph(e);
   void *bufs[] = {e->psi_hat, e->work, e->tw, e->real_buf, e->d_inst, e->flag,
                   e->d_prefix[0], e->d_prefix[1], e->d_prefix[2], e->d_prefix8[0], e->d_prefix8[1],
-                  e->d_prefix8[2]};
+                  e->d_prefix8[2], e->d_order[0], e->d_order[1], e->d_order[2]};
   for (void *p : bufs)
     if (p) cudaFree(p);
   if (e->own_stream && e->stream) cudaStreamDestroy(e->stream);
@@ -325,12 +332,24 @@ int opfc_ensemble_create(int count, const opfc_desc *descs, opfc_ensemble **out)
     std::vector<float> f(twh.begin(), twh.end());
     if (cudaMemcpy(ep->tw, f.data(), f.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) return bail(OPFC_ERR_CUDA);
   }
+  std::vector<int> order[3];
+  for (int st = 0; st < 3; ++st) {
+    auto len = [&](int i) { const EnsInst &in = e->inst[i]; return st == 0 ? in.n1 : (st == 1 ? in.n2 : in.M); };
+    order[st].resize(count);
+    for (int i = 0; i < count; ++i) order[st][i] = i;
+    std::stable_sort(order[st].begin(), order[st].end(), [&](int x, int y) { return len(x) > len(y); });
+    if ((rc = ealloc(ep, (void **)&ep->d_order[st], sizeof(int) * count))) return bail(rc);
+    if (cudaMemcpy(ep->d_order[st], order[st].data(), sizeof(int) * count, cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(OPFC_ERR_CUDA);
+  }
   for (int wi = 0; wi < 2; ++wi) {
     const int W = wi == 0 ? 16 : 8;
     for (int st = 0; st < 3; ++st) {
       std::vector<int> pre(count + 1, 0);
-      for (int i = 0; i < count; ++i)
-        pre[i + 1] = pre[i] + (st < 2 ? col_tiles(e->inst[i], st + 1, W) : x_tiles(e->inst[i], W));
+      for (int k = 0; k < count; ++k) {
+        const EnsInst &in = e->inst[order[st][k]];
+        pre[k + 1] = pre[k] + (st < 2 ? col_tiles(in, st + 1, W) : x_tiles(in, W));
+      }
       ep->total[wi][st] = pre[count];
       int **dst = wi == 0 ? &ep->d_prefix[st] : &ep->d_prefix8[st];
       if ((rc = ealloc(ep, (void **)dst, sizeof(int) * (count + 1)))) return bail(rc);

@@ -28,7 +28,8 @@ struct EnsInst {
 struct EnsArgs {
   const EnsInst *inst;
   int count;
-  const int *prefix;   // tile prefix sums of this stage, count + 1 entries
+  const int *prefix;   // tile prefix sums of this stage, count + 1 entries, in `order`
+  const int *order;    // members in tile order (by line length), or nullptr
   void *work;          // F_z^-1 of the states / the step's working arrays
   void *psi_hat;       // states (DC slot zero)
   const void *tw;      // concatenated twiddle tables
@@ -162,9 +163,9 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_col_kernel(const EnsArgs a, i
   C *pb = sm + 128 * (W + 1);  // z update: psi_hat staging (ens_col_smem)
   const int total = a.prefix[a.count];
   for (int g = blockIdx.x; g < total; g += gridDim.x) {
-    const int i = ens_find(a.prefix, a.count, g);
-    const EnsInst in = a.inst[i];
-    const int t = g - a.prefix[i];
+    const int k = ens_find(a.prefix, a.count, g);
+    const EnsInst in = a.inst[a.order ? a.order[k] : k];
+    const int t = g - a.prefix[k];
     const int N = axis == 1 ? in.n1 : in.n2;
     switch (N) {
       case 16: ens_col_tile<Real, 16, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
@@ -229,9 +230,9 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_x_kernel(const EnsArgs a) {
   const int total = a.prefix[a.count];
   bool bad = false;
   for (int g = blockIdx.x; g < total; g += gridDim.x) {
-    const int i = ens_find(a.prefix, a.count, g);
-    const EnsInst in = a.inst[i];
-    const int t = g - a.prefix[i];
+    const int k = ens_find(a.prefix, a.count, g);
+    const EnsInst in = a.inst[a.order ? a.order[k] : k];
+    const int t = g - a.prefix[k];
     switch (in.M) {
       case 16: ens_x_tile<Real, 16, W>(a, in, t, tw, buf, bad); break;
       case 24: ens_x_tile<Real, 24, W>(a, in, t, tw, buf, bad); break;
