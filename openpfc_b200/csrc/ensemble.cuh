@@ -69,16 +69,23 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 template <typename Real, int N, int W, int MODE, int DIR>
 __device__ __forceinline__ void ens_col_tile(const EnsArgs &a, const EnsInst &in, int axis, int t,
                                              typename Cx<Real>::T *tw, typename Cx<Real>::T *sm,
-                                             typename Cx<Real>::T *pbuf) {
+                                             typename Cx<Real>::T *pbuf, int &tw_cur) {
   using C = typename Cx<Real>::T;
   constexpr int E = N / kEnsT;
   constexpr int ld = W + 1;
   const int tid = threadIdx.x, c = tid % W, j = tid / W;
   const int M = in.M, n1 = in.n1, n2 = in.n2;
   const long long nyq = (long long)M * n1 * n2;
-  const C *gtw = reinterpret_cast<const C *>(a.tw) + (axis == 1 ? in.tw1 : in.tw2);
-  for (int i = tid; i < N; i += W * kEnsT) tw[i] = gtw[i];
-  __syncthreads();
+  // the CTA's previous tile usually had the same length (tiles are walked in
+  // members sorted by length): reload the twiddles only when they change (the
+  // previous tile's closing barrier orders the reuse of the shared arrays)
+  const int two = axis == 1 ? in.tw1 : in.tw2;
+  if (two != tw_cur) {
+    const C *gtw = reinterpret_cast<const C *>(a.tw) + two;
+    for (int i = tid; i < N; i += W * kEnsT) tw[i] = gtw[i];
+    __syncthreads();
+    tw_cur = two;
+  }
   // main segment: columns kx, outer z (y pass) or y (z pass); then the Nyquist plane
   const int ti_main = (M + W - 1) / W;
   const int n_outer = axis == 1 ? n2 : n1;
@@ -162,19 +169,20 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_col_kernel(const EnsArgs a, i
   C *sm = tw + 128;
   C *pb = sm + 128 * (W + 1);  // z update: psi_hat staging (ens_col_smem)
   const int total = a.prefix[a.count];
+  int tw_cur = -1;  // twiddle table offset held in tw
   for (int g = blockIdx.x; g < total; g += gridDim.x) {
     const int k = ens_find(a.prefix, a.count, g);
     const EnsInst in = a.inst[a.order ? a.order[k] : k];
     const int t = g - a.prefix[k];
     const int N = axis == 1 ? in.n1 : in.n2;
     switch (N) {
-      case 16: ens_col_tile<Real, 16, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
-      case 32: ens_col_tile<Real, 32, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
-      case 48: ens_col_tile<Real, 48, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
-      case 64: ens_col_tile<Real, 64, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
-      case 80: ens_col_tile<Real, 80, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
-      case 96: ens_col_tile<Real, 96, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
-      case 128: ens_col_tile<Real, 128, W, MODE, DIR>(a, in, axis, t, tw, sm, pb); break;
+      case 16: ens_col_tile<Real, 16, W, MODE, DIR>(a, in, axis, t, tw, sm, pb, tw_cur); break;
+      case 32: ens_col_tile<Real, 32, W, MODE, DIR>(a, in, axis, t, tw, sm, pb, tw_cur); break;
+      case 48: ens_col_tile<Real, 48, W, MODE, DIR>(a, in, axis, t, tw, sm, pb, tw_cur); break;
+      case 64: ens_col_tile<Real, 64, W, MODE, DIR>(a, in, axis, t, tw, sm, pb, tw_cur); break;
+      case 80: ens_col_tile<Real, 80, W, MODE, DIR>(a, in, axis, t, tw, sm, pb, tw_cur); break;
+      case 96: ens_col_tile<Real, 96, W, MODE, DIR>(a, in, axis, t, tw, sm, pb, tw_cur); break;
+      case 128: ens_col_tile<Real, 128, W, MODE, DIR>(a, in, axis, t, tw, sm, pb, tw_cur); break;
       default: break;  // sizes are validated on the host
     }
   }
@@ -184,7 +192,7 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_col_kernel(const EnsArgs a, i
 template <typename Real, int M, int W>
 __device__ __forceinline__ void ens_x_tile(const EnsArgs &a, const EnsInst &in, int t,
                                            typename Cx<Real>::T *tw, typename Cx<Real>::T *buf,
-                                           bool &bad) {
+                                           bool &bad, int &tw_cur) {
   using C = typename Cx<Real>::T;
   constexpr int E = M / kEnsT;
   constexpr int NT = W * kEnsT;
@@ -193,8 +201,11 @@ __device__ __forceinline__ void ens_x_tile(const EnsArgs &a, const EnsInst &in, 
   const int tid = threadIdx.x, c = tid % W, j = tid / W;
   const int rows = in.n1 * in.n2;
   const long long nyq = (long long)M * rows;
-  const C *gtw = reinterpret_cast<const C *>(a.tw) + in.tw0;
-  for (int i = tid; i < N0; i += NT) tw[i] = gtw[i];
+  if (in.tw0 != tw_cur) {  // made visible by the barrier after the row loads
+    const C *gtw = reinterpret_cast<const C *>(a.tw) + in.tw0;
+    for (int i = tid; i < N0; i += NT) tw[i] = gtw[i];
+    tw_cur = in.tw0;
+  }
   C *work = reinterpret_cast<C *>(a.work) + in.off_c;
   const int row0 = t * W;
   x_load_rows<C, M, W, NT>(work, nyq, row0, rows, buf, tid);
@@ -229,17 +240,18 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_x_kernel(const EnsArgs a) {
   C *buf = tw + 128;
   const int total = a.prefix[a.count];
   bool bad = false;
+  int tw_cur = -1;  // twiddle table offset held in tw
   for (int g = blockIdx.x; g < total; g += gridDim.x) {
     const int k = ens_find(a.prefix, a.count, g);
     const EnsInst in = a.inst[a.order ? a.order[k] : k];
     const int t = g - a.prefix[k];
     switch (in.M) {
-      case 16: ens_x_tile<Real, 16, W>(a, in, t, tw, buf, bad); break;
-      case 24: ens_x_tile<Real, 24, W>(a, in, t, tw, buf, bad); break;
-      case 32: ens_x_tile<Real, 32, W>(a, in, t, tw, buf, bad); break;
-      case 40: ens_x_tile<Real, 40, W>(a, in, t, tw, buf, bad); break;
-      case 48: ens_x_tile<Real, 48, W>(a, in, t, tw, buf, bad); break;
-      case 64: ens_x_tile<Real, 64, W>(a, in, t, tw, buf, bad); break;
+      case 16: ens_x_tile<Real, 16, W>(a, in, t, tw, buf, bad, tw_cur); break;
+      case 24: ens_x_tile<Real, 24, W>(a, in, t, tw, buf, bad, tw_cur); break;
+      case 32: ens_x_tile<Real, 32, W>(a, in, t, tw, buf, bad, tw_cur); break;
+      case 40: ens_x_tile<Real, 40, W>(a, in, t, tw, buf, bad, tw_cur); break;
+      case 48: ens_x_tile<Real, 48, W>(a, in, t, tw, buf, bad, tw_cur); break;
+      case 64: ens_x_tile<Real, 64, W>(a, in, t, tw, buf, bad, tw_cur); break;
       default: break;
     }
   }
