@@ -170,8 +170,13 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_col_kernel(const EnsArgs a, i
   C *pb = sm + 128 * (W + 1);  // z update: psi_hat staging (ens_col_smem)
   const int total = a.prefix[a.count];
   int tw_cur = -1;  // twiddle table offset held in tw
+  int k = -1;  // position (in a.order) of the previous tile's member
   for (int g = blockIdx.x; g < total; g += gridDim.x) {
-    const int k = ens_find(a.prefix, a.count, g);
+    // a CTA's tiles increase, so after the first search the position only advances
+    if (k < 0)
+      k = ens_find(a.prefix, a.count, g);
+    else
+      while (a.prefix[k + 1] <= g) ++k;
     const EnsInst in = a.inst[a.order ? a.order[k] : k];
     const int t = g - a.prefix[k];
     const int N = axis == 1 ? in.n1 : in.n2;
@@ -241,8 +246,13 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_x_kernel(const EnsArgs a) {
   const int total = a.prefix[a.count];
   bool bad = false;
   int tw_cur = -1;  // twiddle table offset held in tw
+  int k = -1;  // position (in a.order) of the previous tile's member
   for (int g = blockIdx.x; g < total; g += gridDim.x) {
-    const int k = ens_find(a.prefix, a.count, g);
+    // a CTA's tiles increase, so after the first search the position only advances
+    if (k < 0)
+      k = ens_find(a.prefix, a.count, g);
+    else
+      while (a.prefix[k + 1] <= g) ++k;
     const EnsInst in = a.inst[a.order ? a.order[k] : k];
     const int t = g - a.prefix[k];
     switch (in.M) {
