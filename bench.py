@@ -38,7 +38,7 @@ N = 512
 DX = [math.pi / 4] * 3
 DT, R, N0, AMP, SEED = 0.5, -0.25, -0.285, 0.01, 7
 METRIC = "Mcell-steps/s at 512^3 FP32 vs FP64 GPU (<=1e-5 rel-L2); FFT-pass HBM % of peak"
-WORKLOAD = "plain conserved PFC 512^3, FP32 bulk / FP64 tables, dx=pi/4 dt=0.5 r=-0.25"
+WORKLOAD = "plain conserved PFC 512^3, FP32 bulk, dx=pi/4 dt=0.5 r=-0.25"
 
 
 def peaks():
@@ -58,18 +58,56 @@ def dist():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during a region."""
+    """SM clocks and throttle reasons sampled during a region: NVML polled every
+    few milliseconds from a thread (read-only queries), or nvidia-smi where the
+    NVML binding is missing."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clocks-event reason bits
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40}
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period_s: float = 0.002):
         self.device = device
+        self.period = period_s
         self.p = None
+        self.nv = None
+        self.samples = []  # (sm_mhz, max_mhz, reasons bitmask)
+        self.lines = []
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uid = "GPU-" + str(torch.cuda.get_device_properties(self.device).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
     def __enter__(self):
         import threading
-        self.lines = []
+        self.stop = threading.Event()
+        try:
+            nv, h = self._nvml_handle()
+            reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+
+            def poll():
+                while not self.stop.is_set():
+                    try:
+                        self.samples.append((nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM), smax, reasons(h)))
+                    except Exception:
+                        pass
+                    time.sleep(self.period)
+
+            self.nv = nv
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            return self
+        except Exception:
+            self.nv = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                        "-i", str(self.device), "-lms", "100"],
@@ -92,6 +130,9 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        self.stop.set()
+        if self.nv is not None:
+            self.t.join(timeout=2)
         if self.p:
             time.sleep(0.15)
             self.p.terminate()
@@ -103,8 +144,14 @@ class Clocks:
 
     def summary(self):
         sm, smax, reasons = [], None, set()
+        for mhz, mx, bits in self.samples:
+            sm.append(float(mhz))
+            smax = float(mx)
+            for nm, b in self.BITS.items():
+                if int(bits) & b:
+                    reasons.add(nm)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for l in getattr(self, "lines", []):
+        for l in self.lines:
             f = [x.strip() for x in l.split(",")]
             if len(f) < 9:
                 continue
@@ -117,29 +164,49 @@ class Clocks:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "source": "nvml" if self.samples else ("nvidia-smi" if self.lines else None)}
 
 
-def z_tables(var_z, t):
-    """Per-mode operator tables the z-update variant streams from HBM: t for the
-    table variants (0, 2), none when the operators come from the L2-resident
-    radial table (1) or are computed from k^2 (3, 4)."""
-    return t if var_z in (0, 2) else 0
+# z-update variants (opfc_autotune): 0/2 stream per-mode FP64-built tables,
+# 1 radial FP64-built tables (L2), 3-5 compute opL/opN per mode in the compute
+# precision, 6-8 read the folded FP64-built tables
+def operator_source(var_z):
+    if var_z in (3, 4, 5):
+        return "opL/opN computed per mode in the compute precision (expm1f, fast divide)"
+    if var_z in (6, 7, 8):
+        return "FP64-built opL/opN tables rounded to FP32 (folded by the evenness of k^2 in ky, kz)"
+    if var_z == 1:
+        return "FP64-built opL/opN radial tables rounded to FP32"
+    return "FP64-built per-mode opL/opN tables rounded to FP32"
 
 
-def alg_bytes_per_kernel(n, prec_bytes, tables=2):
+def z_table_bytes(var_z, n, t, st):
+    """HBM bytes of operator tables one z update reads: t per-mode tables for
+    the table variants (0, 2); the folded tables, (M+1)(N/2+1)^2 modes read once
+    per step (tiles walked in (ky, N - ky) pairs), for 6-8; none for the radial
+    (L2-resident) and computed variants."""
+    if var_z in (0, 2):
+        return (n // 2 + 1) * n * n * t * st
+    if var_z in (6, 7, 8):
+        return (n // 2 + 1) * (n // 2 + 1) * (n // 2 + 1) * t * st
+    return 0
+
+
+def alg_bytes_per_kernel(n, prec_bytes, table_bytes):
     """Algorithmic HBM bytes per launch of each kernel of the plain step: every
     pass reads and writes each complex mode once; the z update also reads and
-    writes psi_hat and reads `tables` per-mode operator tables."""
+    writes psi_hat and reads `table_bytes` of operator tables."""
     nc = (n // 2 + 1) * n * n
-    sc, st = 2 * prec_bytes, prec_bytes
+    sc = 2 * prec_bytes
     return {"y_inverse": 2 * nc * sc, "x_fused": 2 * nc * sc, "y_forward": 2 * nc * sc,
-            "z_update": nc * (4 * sc + tables * st), "hermitian_fix": 4 * 2 * n * n * sc}
+            "z_update": nc * 4 * sc + table_bytes, "hermitian_fix": 4 * 2 * n * n * sc}
 
 
 def cpu_baseline(psi0, budget_s=30.0):
     """Time the FP64 C restatement of the reference step on all host threads."""
     from oracle import oracle as O
+    O.set_threads(len(os.sched_getaffinity(0)))
     threads = O.get_threads()
     psi = np.ascontiguousarray(psi0, dtype=np.float64).copy()
     t1 = O.time_plain(psi, DX, R, DT, 1)
@@ -156,52 +223,66 @@ def cpu_baseline(psi0, budget_s=30.0):
 
 
 def run_reference(args):
+    """The reference algorithm's CPU path on this host's cores: the FP64 C
+    restatement of the plain PFC step (the reference's own FFTW/HeFFTe/MPI build
+    cannot be built here), on the same 512^3 workload and initial condition (the
+    oracle's noise generator equals the product's bit for bit).  Nothing of the
+    product package is imported in this process.  W untimed warm-up steps, then
+    up to K timed steps bounded to ~150 s."""
     ws, rank, _ = dist()
     if rank != 0:
         return 0
-    import ctypes  # noqa: F401
     from oracle import oracle as O
-    import openpfc_b200 as ob
-    psi = ob.ic_noise((N, N, N), N0, AMP, SEED)
+    # every host thread this process may run on (torchrun sets OMP_NUM_THREADS=1)
+    O.set_threads(len(os.sched_getaffinity(0)))
+    psi = O.ic_noise((N, N, N), N0, AMP, SEED)
     threads = O.get_threads()
-    # bounded sample: one untimed step when affordable, then as many of the
-    # requested steps as fit in ~150 s
-    t1 = O.time_plain(psi, DX, R, DT, 1)
+    t1 = O.time_plain(psi, DX, R, DT, 1)  # first step: paging and thread start-up
+    w = max(0, min(args.warmup - 1, int(60.0 / max(t1, 1e-9))))
+    if w:
+        O.time_plain(psi, DX, R, DT, w)
     k = max(1, min(args.steps, int(150.0 / max(t1, 1e-9))))
     t = O.time_plain(psi, DX, R, DT, k)
     v = psi.size * k / t / 1e6
-    line = {"metric": METRIC, "value": v, "unit": "Mcell-steps/s", "n_gpus": args.gpus,
-            "steps": k, "warmup": 1, "ms_per_step": 1e3 * t / k, "higher_is_better": True,
+    line = {"metric": METRIC, "value": v, "unit": "Mcell-steps/s", "n_gpus": 0, "host_threads": threads,
+            "steps": k, "warmup": 1 + w, "ms_per_step": 1e3 * t / k, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD.replace("FP32 bulk / FP64 tables", "FP64 CPU"),
+            "config": {"workload": f"plain conserved PFC {N}^3, FP64 CPU, dx=pi/4 dt=0.5 r=-0.25",
                        "n": N, "l2": "arrays larger than L2"},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "Mcell-steps/s", "cores": threads, "kind": "port",
-                             "sample": f"{k} plain PFC steps at {N}^3 FP64, C restatement of the "
-                                       f"reference path (FFTW/HeFFTe/MPI absent), {threads} threads"},
+                             "sample": f"{k} plain PFC steps at {N}^3 FP64 after {1 + w} warm-up step(s), "
+                                       f"C restatement of the reference path (FFTW/HeFFTe/MPI absent), "
+                                       f"{threads} threads"},
             "e2e": {"value": v, "unit": "Mcell-steps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-def timed_steps(model, steps, warmup, ws, stream):
+def timed_steps(model, steps, warmup, ws, stream, repeats=1):
+    """W warm-up steps, then `repeats` timed regions of exactly `steps` steps,
+    each bracketed by a barrier and a device synchronize and timed with CUDA
+    events on the handle's stream; returns (median ms, all ms), max over ranks."""
     import torch
+    from openpfc_b200.parallel_plan import max_over_ranks
     model.step(warmup)
     model.sync()
-    if ws > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    model.step(steps)
-    e1.record(stream)
-    e1.synchronize()
-    model.sync()
-    torch.cuda.synchronize()
-    from openpfc_b200.parallel_plan import max_over_ranks
-    return max_over_ranks(e0.elapsed_time(e1), device="cuda")
+    times = []
+    for _ in range(repeats):
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        model.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        model.sync()
+        torch.cuda.synchronize()
+        times.append(max_over_ranks(e0.elapsed_time(e1), device="cuda"))
+    return statistics.median(times), times
 
 
 def run_b200(args):
@@ -227,7 +308,7 @@ def run_b200(args):
     stream = torch.cuda.ExternalStream(m.stream, device=torch.device("cuda", local))
     # clocks are sampled from the warm-up through the end of the timed region
     with Clocks(local) as ck:
-        ms = timed_steps(m, args.steps, args.warmup, ws, stream)
+        ms, reps_ms = timed_steps(m, args.steps, args.warmup, ws, stream, repeats=args.repeats)
     value = ws * cells * args.steps / (ms / 1e3) / 1e6
     kps = m.kernels_per_step()
 
@@ -239,8 +320,8 @@ def run_b200(args):
         m64.autotune()
         m64.set_psi(psi0_32.astype(np.float64))
         s64 = max(3, min(args.steps, 20))
-        ms64 = timed_steps(m64, s64, min(args.warmup, 3), ws, torch.cuda.ExternalStream(
-            m64.stream, device=torch.device("cuda", local)))
+        ms64, _ = timed_steps(m64, s64, min(args.warmup, 3), ws, torch.cuda.ExternalStream(
+            m64.stream, device=torch.device("cuda", local)), repeats=3)
         v64 = ws * cells * s64 / (ms64 / 1e3) / 1e6
         extra["fp64"] = {"value": v64, "ms_per_step": ms64 / s64, "steps": s64}
         extra["fp32_over_fp64"] = value / v64
@@ -291,7 +372,7 @@ def run_b200(args):
     # per-kernel device time (each kernel alone, CUDA events on the handle's stream)
     m.set_psi(psi0_32)
     prof = m.profile_step(reps=args.profile_reps)
-    ab = alg_bytes_per_kernel(N, 4, z_tables(m.variants()[2], 2))
+    ab = alg_bytes_per_kernel(N, 4, z_table_bytes(m.variants()[2], N, 2, 4))
     passes = {}
     for k, t in prof.items():
         gbs = ab[k] / (t / 1e3) / 1e9
@@ -323,10 +404,12 @@ def run_b200(args):
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "n": N, "per_gpu_cells": cells,
+                "config": {"workload": WORKLOAD, "operators": operator_source(m.variants()[2]),
+                           "n": N, "per_gpu_cells": cells,
                            "l2": "inputs larger than L2 (0.54 GB arrays), no flush",
                            "parallelism": f"replicas x{ws}"},
                 "e2e": e2e, "roofline": roofline, "passes": passes, "cpu_baseline": cpu,
+                "timing": {"repeats": len(reps_ms), "ms_each": reps_ms, "value_from": "median"},
                 "clocks": ck.summary(), "gpu_launches": kps * args.steps,
                 "autotune": {"variants_yxz": m.variants(), "ms": tune32}}
         line.update(extra)
@@ -354,12 +437,12 @@ def run_filtered(args):
     del psi0
     stream = torch.cuda.ExternalStream(m.stream)
     with Clocks(0) as ck:
-        ms = timed_steps(m, args.steps, args.warmup, 1, stream)
+        ms, _ = timed_steps(m, args.steps, args.warmup, 1, stream, repeats=args.repeats)
     cells = n ** 3
     nc = (n // 2 + 1) * n * n
     prof = m.profile_step(reps=max(2, args.profile_reps // 2))
     ab = {"y_inverse": 16 * nc, "x_fused": 16 * nc, "y_forward": 16 * nc,
-          "z_update": nc * (32 + 4 * z_tables(m.variants()[2], 3)), "hermitian_fix": 4 * 2 * n * n * 8}
+          "z_update": nc * 32 + z_table_bytes(m.variants()[2], n, 3, 4), "hermitian_fix": 4 * 2 * n * n * 8}
     passes = {k: {"ms": t, "gbs": ab[k] / (t / 1e3) / 1e9, "frac": ab[k] / (t / 1e3) / 1e9 / hbm}
               for k, t in prof.items()}
     line = {"metric": "Mcell-steps/s, filtered PFC 1024^3 FP32", "value": cells * args.steps / (ms / 1e3) / 1e6,
@@ -447,13 +530,52 @@ def run_ensemble(args):
     return 0
 
 
+def relaunch_under_torchrun(args, argv):
+    """`--gpus N` with N > 1 outside torchrun: re-run this script as N ranks
+    (one per GPU, or per CPU process with --dry-run) on this node and return
+    the launcher's exit status.  Rank 0 prints the JSON line."""
+    import socket
+    with socket.socket() as so:  # a free rendezvous port on the loopback address
+        so.bind(("127.0.0.1", 0))
+        port = so.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr=127.0.0.1", f"--master-port={port}", os.path.abspath(__file__)] + list(argv)
+    return subprocess.call(cmd)
+
+
+def run_dry(args):
+    """The launcher without the GPU work: every rank joins a gloo process group,
+    the ranks agree on the world size and rank 0 prints the line it would print
+    (value 0).  Tests the multi-process path on a machine without GPUs."""
+    import datetime
+    import torch
+    import torch.distributed as tdist
+    ws, rank, _ = dist()
+    if ws > 1:
+        tdist.init_process_group("gloo", timeout=datetime.timedelta(seconds=60))
+        t = torch.tensor([1.0])
+        tdist.all_reduce(t)
+        ranks = int(t.item())
+        tdist.destroy_process_group()
+    else:
+        ranks = 1
+    if rank == 0:
+        print(json.dumps({"metric": METRIC, "value": 0.0, "unit": "Mcell-steps/s", "n_gpus": ranks,
+                          "dry_run": True, "scaling": "weak",
+                          "config": {"workload": WORKLOAD, "parallelism": f"replicas x{ranks}"}}), flush=True)
+    return 0
+
+
 def main(argv=None):
+    argv = sys.argv[1:] if argv is None else argv
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--n", type=int, default=512,
                     help="grid side (512 is the measured workload; smaller sides are for profiling)")
     ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--repeats", type=int, default=5,
+                    help="timed regions of --steps steps each; value is their median")
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -464,13 +586,20 @@ def main(argv=None):
     ap.add_argument("--workload", default="plain", choices=["plain", "filtered", "ensemble"],
                     help="plain: the measured 512^3 line; filtered: mean-field-filtered 1024^3 FP32; "
                          "ensemble: 256 uneven members, 50 steps in one graph")
+    ap.add_argument("--dry-run", action="store_true",
+                    help="launch the ranks and print the line without GPU work (gloo; for tests)")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
+    args.repeats = max(1, args.repeats)
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return relaunch_under_torchrun(args, argv)
     global N, WORKLOAD
     if args.n != N:
         WORKLOAD = WORKLOAD.replace(f"{N}^3", f"{args.n}^3")
         N = args.n
+    if args.dry_run:
+        return run_dry(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.workload == "filtered":

@@ -131,6 +131,15 @@ int opfc_step(opfc_handle *h, int n_steps);
  * produced NaN/Inf since the last check. */
 int opfc_sync(opfc_handle *h);
 
+/* Failure-path check (no reference counterpart; the reference's GPU model
+ * blocks in cudaDeviceSynchronize without a limit): runs the bounded mbarrier
+ * wait that every pipelined pass kernel uses on a barrier that nothing
+ * completes, with a limit of limit_ms (0.1 .. 1000, the passes use 4 s).  The
+ * wait expires, the kernel records the timeout in the handle's status flag and
+ * returns, and the next opfc_sync reports OPFC_ERR_TIMEOUT; the handle stays
+ * usable.  No fault is raised and no copy is left in flight. */
+int opfc_check_bounded_wait(opfc_handle *h, double limit_ms);
+
 /* Stand-alone transforms with the reference's IFFT contract
  * (include/openpfc/kernel/fft/fft_interface.hpp:51,61): forward R2C
  * unnormalised, backward C2R scaled by 1/(N0 N1 N2).  Buffers as above. */
@@ -174,14 +183,22 @@ const char *opfc_step_kernel_name(int k);
  * 0 pipelined with streamed tables | 1 pipelined with radial tables (isotropic
  * grids) | 2 direct with streamed tables | 3 pipelined with operators computed
  * from k^2 | 4 direct with computed operators | 5 as 3 with ping-pong exchange
- * buffers (3-5: PLAIN and FILTERED);
+ * buffers (3-5: PLAIN and FILTERED) | 6 pipelined with the folded tables and
+ * ping-pong exchange buffers | 7 direct with the folded tables | 8 pipelined
+ * with the folded tables (6-8: every model but the moving-gradient Aluminum
+ * and caller-supplied operators);
  * 3 warm-up + 10 timed launches each), keeps the fastest and caches it per
- * device; opfc_initialize applies cached choices.  ms (OPFC_AUTOTUNE_SLOTS
- * doubles, may be NULL) receives the mean milliseconds per launch of
- * y0 .. y4 x0 .. x3 z0 .. z5 (-1 if not applicable).  Call after
- * opfc_initialize; the passes run in place, so set the field afterwards.
- * opfc_variants reports the chosen (y, x, z) variants. */
-#define OPFC_AUTOTUNE_SLOTS 15
+ * device; opfc_initialize applies cached choices.  Every table variant holds
+ * operators built in FP64 on the host and rounded once to the compute
+ * precision (the folded tables hold the per-mode values of the modes
+ * (kx, |ky|, |kz|), k^2 being even in ky and kz); the computed variants 3-5
+ * evaluate them per mode in the compute precision, so FP32 handles consider
+ * them only with OPFC_FP32_COMPUTED_OPERATORS=1 in the environment.
+ * ms (OPFC_AUTOTUNE_SLOTS doubles, may be NULL) receives the mean
+ * milliseconds per launch of y0 .. y4 x0 .. x3 z0 .. z8 (-1 if not applicable).
+ * Call after opfc_initialize; the passes run in place, so set the field
+ * afterwards.  opfc_variants reports the chosen (y, x, z) variants. */
+#define OPFC_AUTOTUNE_SLOTS 18
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 
@@ -264,6 +281,16 @@ int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, do
  * reference's order (the standard library's mapping, as in the reference). */
 int opfc_ic_seed_grid_fcc(double *psi, const int n[3], const double dx[3], const double origin[3], int Nx, int Ny,
                           int Nz, double X0, double radius, double amplitude, double rho, double rseed);
+/* opfc_ic_random_seeds: the reference's RandomSeeds initial condition
+ * (include/openpfc/kernel/simulation/initial_conditions/random_seeds.hpp:54-101,
+ * with Seed of seed.hpp): 150 seeds of radius 20 placed in the reference's
+ * fixed box (x in [-108, -68), y, z in [-128, 128)) and rotated at random, from
+ * std::mt19937_64(42) through std::uniform_real_distribution in the
+ * reference's order; a cell inside a seed takes density + sum_q 2 amplitude
+ * cos(q.x) over the six rotated <110>/sqrt(2) vectors (the first seed that
+ * contains it wins), every other cell 0.  The whole field is written. */
+int opfc_ic_random_seeds(double *psi, const int n[3], const double dx[3], const double origin[3], double density,
+                         double amplitude);
 
 /* On-disk formats of the reference's writers and readers (one process owns
  * the whole grid; no MPI).
@@ -292,13 +319,19 @@ int opfc_read_binary(opfc_handle *h, const char *filename);
 int opfc_write_vti(opfc_handle *h, const char *pattern, int increment, const char *field_name);
 /* The same formats for host arrays and one process's box of a global grid
  * (x fastest; box = local extent at offset, as set_domain(global, local,
- * offset) of the reference's writers): opfc_write_raw truncates `filename`
- * and writes the box of `ncomp` (1 real, 2 complex) doubles per point at its
- * place in the global array; opfc_read_raw reads such a box (short file ->
- * OPFC_ERR_SIZE); opfc_write_vti_raw writes one .vti piece.  A box outside
- * the grid -> OPFC_ERR_ARG. */
+ * offset) of the reference's writers): opfc_write_raw writes the box of
+ * `ncomp` (1 real, 2 complex) doubles per point at its place in the global
+ * array -- a box covering the whole grid truncates `filename` first, a smaller
+ * box is written in place (the file is created if missing, never truncated), so
+ * that several writers can each fill their own box of one file;
+ * opfc_prepare_raw truncates `filename` and sizes it to the whole grid, the
+ * one-time step before such writers (the reference's collective
+ * MPI_File_set_size(fh, 0), binary_writer.hpp); opfc_read_raw reads a box
+ * (short file -> OPFC_ERR_SIZE); opfc_write_vti_raw writes one .vti piece.  A
+ * box outside the grid -> OPFC_ERR_ARG. */
 int opfc_write_raw(const char *filename, const int global[3], const int local[3], const int offset[3],
                    const double *data, int ncomp);
+int opfc_prepare_raw(const char *filename, const int global[3], int ncomp);
 int opfc_read_raw(const char *filename, const int global[3], const int local[3], const int offset[3],
                   double *data, int ncomp);
 int opfc_write_vti_raw(const char *filename, const int global[3], const int local[3], const int offset[3],
@@ -306,11 +339,13 @@ int opfc_write_vti_raw(const char *filename, const int global[3], const int loca
 
 /* Forward R2C transform that allocates nothing (no counterpart in the
  * reference; it is opfc_fft_forward without a handle).  For callers that cannot
- * call cudaMalloc -- code inside CUDA graph capture, allocation-free real-time
- * loops, hosts whose memory manager owns every device allocation.  in_real and
- * out_complex are device pointers of the given precision (OPFC_FP32/OPFC_FP64)
- * in the boundary layout above; the work is queued on `stream` (NULL = legacy
- * default stream) and the call does not wait for it.
+ * call cudaMalloc: latency-bound loops, where cudaMalloc's implicit device-wide
+ * synchronisation and unbounded run time are not acceptable, and host
+ * applications whose own memory manager owns every device allocation and does
+ * not let a library allocate.  in_real and out_complex are device pointers of
+ * the given precision (OPFC_FP32/OPFC_FP64) in the boundary layout above; the
+ * work is queued on `stream` (NULL = legacy default stream) and the call does
+ * not wait for it.
  * The intermediate half spectrum lives in a fixed 16 MiB device array inside
  * the library (held by every GPU that loads it until exit):
  * (N0/2+1)*N1*N2 * (8 bytes FP32 | 16 bytes FP64) must be <= 16 MiB and every

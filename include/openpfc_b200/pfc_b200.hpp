@@ -454,6 +454,14 @@ class DomainIO {
 class BinaryWriter : public DomainIO {
  public:
   using DomainIO::DomainIO;
+  /// Truncate the file of `increment` and size it to the global array: the
+  /// one-time step before several writers each write their own box (the
+  /// reference does it collectively with MPI_File_set_size(fh, 0)).  A writer
+  /// whose box is the whole array truncates by itself.
+  void prepare(int increment, int ncomp = 1) {
+    const std::string fn = format_with_number(filename_, increment);
+    check(opfc_prepare_raw(fn.c_str(), global_.data(), ncomp), "BinaryWriter::prepare", fn.c_str());
+  }
   void write(int increment, const std::vector<double> &data) {
     expect("BinaryWriter::write", data.size());
     const std::string fn = format_with_number(filename_, increment);

@@ -232,7 +232,8 @@ class _ModelBase(_Handle):
         names = ["y.pipelined", "y.direct", "y.narrow", "y.pingpong", "y.direct_e32", "x.pipelined", "x.direct",
                  "x.no_square",
                  "x.square_direct",
-                 "z.tables", "z.radial", "z.direct", "z.computed", "z.direct_computed", "z.computed_pingpong"]
+                 "z.tables", "z.radial", "z.direct", "z.computed", "z.direct_computed", "z.computed_pingpong",
+                 "z.folded_pingpong", "z.direct_folded", "z.folded"]
         ms = (ctypes.c_double * len(names))()
         _check(self._h, lib().opfc_autotune(self._h, ms))
         return dict(zip(names, list(ms)))
@@ -423,6 +424,17 @@ def ic_seed_grid_fcc(psi: np.ndarray, dx, origin, Nx, Ny, Nz, X0, radius, amplit
                                      float(X0), float(radius), float(amplitude), float(rho), float(rseed))
     if rc != 0:
         raise ValueError(f"opfc_ic_seed_grid_fcc: {rc}")
+    return out
+
+
+def ic_random_seeds(n, dx, origin, density, amplitude) -> np.ndarray:
+    """RandomSeeds (include/openpfc/kernel/simulation/initial_conditions/
+    random_seeds.hpp): 150 rotated one-mode BCC seeds of radius 20 drawn from
+    std::mt19937_64(42) in the reference's fixed box, 0 outside them; returns a
+    (N2, N1, N0) field."""
+    out = np.zeros((n[2], n[1], n[0]))
+    _check(None, lib().opfc_ic_random_seeds(_dp(out), _i3(n), _d3(dx), _d3(origin), float(density),
+                                            float(amplitude)))
     return out
 
 

@@ -117,6 +117,7 @@ def lib():
     L.opfc_ic_seed.argtypes = [dp, ip, dp, dp, dp, cd, cd, cd, ci]
     L.opfc_ic_seeds.argtypes = [dp, ip, dp, cd, cd, ci, cd, cd, ctypes.c_uint64]
     L.opfc_ic_seed_grid_fcc.argtypes = [dp, ip, dp, dp, ci, ci, ci, cd, cd, cd, cd, cd]
+    L.opfc_ic_random_seeds.argtypes = [dp, ip, dp, dp, cd, cd]
     L.opfc_fft_forward_noalloc.argtypes = [vp, vp, ip, ci, vp]
     cp = ctypes.c_char_p
     L.opfc_format_filename.argtypes = [cp, ci, ctypes.c_char_p, sz]
@@ -128,6 +129,7 @@ def lib():
     L.opfc_set_operators.argtypes = [H, dp, dp, dp, sz]
     L.opfc_write_raw.argtypes = [cp, ip, ip, ip, dp, ci]
     L.opfc_read_raw.argtypes = [cp, ip, ip, ip, dp, ci]
+    L.opfc_prepare_raw.argtypes = [cp, ip, ci]
     L.opfc_write_vti_raw.argtypes = [cp, ip, ip, ip, dp, dp, cp, dp]
     L.opfc_ensemble_create.argtypes = [ci, ctypes.POINTER(Desc), ctypes.POINTER(H)]
     L.opfc_ensemble_destroy.argtypes = [H]
@@ -145,6 +147,7 @@ def lib():
     L.opfc_ensemble_stream.argtypes = [H]
     L.opfc_ensemble_stream.restype = vp
     L.opfc_autotune.argtypes = [H, dp]
+    L.opfc_check_bounded_wait.argtypes = [H, cd]
     L.opfc_variants.argtypes = [H, ip]
     L.opfc_set_r.argtypes = [H, cd]
     L.opfc_forward_checkpointed.argtypes = [H, ci, ci]

@@ -5,7 +5,8 @@
 // default, tune() times every candidate (3 warm-up runs, then 10 timed runs,
 // here with CUDA events on the caller's stream) and stores the fastest; the cache
 // lives in $OPENPFC_GPU_AUTOTUNE_CACHE_DIR (default ".") as
-// <device id>_opfc_autotune.json.  OPENPFC_GPU_AUTOTUNE_DISABLE=1 always returns
+// <device id>_opfc_autotune.json, one file and one in-memory table per device
+// (the device current at the call).  OPENPFC_GPU_AUTOTUNE_DISABLE=1 always returns
 // defaults; OPENPFC_GPU_AUTOTUNE_MODE = auto | cache_only | fallback_only.
 // Where the reference tunes 1D block sizes of finite-difference kernels, the
 // candidates here are FFT tile shapes and kernel families.
@@ -36,9 +37,9 @@ class AutoTuner {
     std::lock_guard<std::mutex> lock(mu_);
     refresh();
     if (disabled_ || mode_ == "fallback_only") return fallback;
-    load_once();
-    auto it = cache_.find(key);
-    return it == cache_.end() ? fallback : it->second.first;
+    const Table &t = table();
+    auto it = t.entries.find(key);
+    return it == t.entries.end() ? fallback : it->second.first;
   }
 
   // time `run(v)` for v in [0, n) on `s`; cache and return the fastest.
@@ -81,9 +82,9 @@ class AutoTuner {
     cudaEventDestroy(e1);
     if (best < 0) return 0;
     std::lock_guard<std::mutex> lock(mu_);
-    load_once();
-    cache_[key] = {best, best_ms};
-    save();
+    Table &t = table();
+    t.entries[key] = {best, best_ms};
+    save(t);
     return best;
   }
 
@@ -100,10 +101,14 @@ class AutoTuner {
     const std::string dir = c ? c : ".";
     if (dir != dir_) {
       dir_ = dir;
-      loaded_ = false;
-      cache_.clear();
+      tables_.clear();
     }
   }
+
+  struct Table {
+    std::string path;
+    std::map<std::string, std::pair<int, double>> entries;
+  };
 
   std::string path() const {
     int dev = 0;
@@ -116,37 +121,42 @@ class AutoTuner {
     return dir_ + "/" + id + "_opfc_autotune.json";
   }
 
-  // one entry per line: "key": [variant, ms],
-  void load_once() {
-    if (loaded_) return;
-    loaded_ = true;
-    std::ifstream f(path());
+  // the current device's table, read from its file on first use; one entry per
+  // line: "key": [variant, ms],
+  Table &table() {
+    const std::string p = path();
+    auto it = tables_.find(p);
+    if (it != tables_.end()) return it->second;
+    Table &t = tables_[p];
+    t.path = p;
+    std::ifstream f(p);
     std::string line;
     while (std::getline(f, line)) {
       const auto q0 = line.find('"'), q1 = line.find('"', q0 + 1), b = line.find('[', q1);
       if (q0 == std::string::npos || q1 == std::string::npos || b == std::string::npos) continue;
       int v = 0;
       double ms = 0;
-      if (std::sscanf(line.c_str() + b, "[%d, %lf]", &v, &ms) == 2) cache_[line.substr(q0 + 1, q1 - q0 - 1)] = {v, ms};
+      if (std::sscanf(line.c_str() + b, "[%d, %lf]", &v, &ms) == 2) t.entries[line.substr(q0 + 1, q1 - q0 - 1)] = {v, ms};
     }
+    return t;
   }
 
-  void save() {
-    std::ofstream f(path());
+  static void save(const Table &t) {
+    std::ofstream f(t.path);
     if (!f) return;
     f << "{\n";
     size_t i = 0;
-    for (const auto &kv : cache_) {
+    for (const auto &kv : t.entries) {
       f << " \"" << kv.first << "\": [" << kv.second.first << ", " << kv.second.second << "]"
-        << (++i < cache_.size() ? ",\n" : "\n");
+        << (++i < t.entries.size() ? ",\n" : "\n");
     }
     f << "}\n";
   }
 
   std::mutex mu_;
-  bool disabled_ = false, loaded_ = false;
+  bool disabled_ = false;
   std::string mode_, dir_;
-  std::map<std::string, std::pair<int, double>> cache_;
+  std::map<std::string, Table> tables_;  // by cache file (one per device)
 };
 
 }  // namespace opfc

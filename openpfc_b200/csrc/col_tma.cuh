@@ -44,8 +44,10 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Wait for phase `parity` of `bar`; false after ~4 s.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
+// Wait for phase `parity` of `bar`; false after limit_ns of %globaltimer (4 s
+// in the pass kernels).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity,
+                                          unsigned long long limit_ns = 4000000000ull) {
   const unsigned a = smem_u32(bar);
   unsigned long long t0 = 0;
   for (unsigned i = 0;; ++i) {
@@ -59,7 +61,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity) {
     if (ok) return true;
     if (i == 0)
       t0 = global_ns();
-    else if ((i & 31u) == 0 && global_ns() - t0 > 4000000000ull)
+    else if ((i & 31u) == 0 && global_ns() - t0 > limit_ns)
       return false;
   }
 }
@@ -83,10 +85,15 @@ struct TmaCfg {
   static constexpr bool CHI = UPD && MODEL != MK_PLAIN;
   static constexpr size_t TILE_C = size_t(N) * W * sizeof(C);
   static constexpr size_t TILE_R = size_t(N) * W * sizeof(Real);
+  // folded tables (OPS 3): rows |kz| = 0 .. N/2 of the tile's columns, as 3
+  // boxes of RBF = N/4 rows of (opL, opN) pairs (and of the filter)
+  static constexpr int RBF = N / 4;
+  static constexpr size_t FOLD_C = 3 * size_t(RBF) * W * sizeof(C);
+  static constexpr size_t FOLD = FOLD_C + (CHI ? 3 * size_t(RBF) * W * sizeof(Real) : 0);
   // radial operators come from an L2-resident table and computed operators
-  // from k^2: only the per-mode tables are staged
+  // from k^2: only the per-mode and the folded tables are staged
   static constexpr size_t STAGE =
-      TILE_C + (UPD ? TILE_C + (OPS != 0 ? 0 : 2 * TILE_R + (CHI ? TILE_R : 0)) : 0);
+      TILE_C + (UPD ? TILE_C + (OPS == 0 ? 2 * TILE_R + (CHI ? TILE_R : 0) : OPS == 3 ? FOLD : 0) : 0);
   static constexpr size_t TW = align128(size_t(N) * sizeof(C));
   // PP: a second FFT exchange buffer (ping-pong with the landed tile)
   static constexpr size_t XB = PP ? align128(TILE_C) : 0;
@@ -125,9 +132,18 @@ __device__ __forceinline__ void upd_fft(C (&x)[Plan<N>::E], C *buf, int ld, int 
     fft_line<C, N, D, N>(x, buf, ld, c, j, tw);
 }
 
+// Outer index (ky of a z tile) of the o-th tile row in the order
+// 0, 1, n-1, 2, n-2, ...: the rows ky and n - ky, which read the same folded
+// table rows, follow each other, so the second read hits L2.  A bijection of
+// [0, n).
+__device__ __forceinline__ int paired_outer(int o, int n) {
+  return o == 0 ? 0 : ((o & 1) ? (o + 1) / 2 : n - o / 2);
+}
+
 // Tensor maps: PLAIN uses m0 (array set 0) and m1 (array set 1); UPDATE uses
 // m0 = N_hat partial (A), m1 = psi_hat, m2 = tab_a, m3 = tab_b, m4 = tab_chi
-// (m2..m4 unused unless OPS == 0, per-mode tables).  MINB CTAs share an SM.
+// (m2..m4 unused unless OPS == 0, per-mode tables); with OPS == 3, m2 = the
+// folded (opL, opN) pairs and m3 = the folded filter.  MINB CTAs share an SM.
 template <typename Real, int N, int W, int MODE, int DIR, int MODEL, bool INV, int OPS, int MINB, bool PP>
 __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
     col_tma_kernel(const __grid_constant__ CUtensorMap m0, const __grid_constant__ CUtensorMap m1,
@@ -138,6 +154,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
   using C = typename Cx<Real>::T;
   constexpr bool RADIAL = OPS == 1;
   constexpr bool COMPUTED = OPS == 2;
+  constexpr bool FOLDED = OPS == 3;
   constexpr int E = Plan<N>::E;
   constexpr int T = N / E;
   constexpr int NT = W * T;
@@ -170,9 +187,12 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
   const ColSeg sg = a.seg0;
   const int ntm = sg.ntiles;
   const int G = gridDim.x;
+  // FOLDED walks the z tiles' ky in (ky, N1 - ky) pairs
+  const int nout = sg.tiles_inner > 0 ? ntm / sg.tiles_inner : 0;
+  auto outer = [&](int o) { return FOLDED ? paired_outer(o, nout) : o; };
 
   auto issue = [&](int s, int t) {
-    const int ti = t % sg.tiles_inner, to = t / sg.tiles_inner;
+    const int ti = t % sg.tiles_inner, to = outer(t / sg.tiles_inner);
     unsigned char *st = stage0 + s * Cfg::STAGE;
     mbar_expect_tx(&bars[s], (unsigned)Cfg::STAGE);
 #pragma unroll
@@ -189,6 +209,19 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
         tma_load_3d(st + 2 * Cfg::TILE_C + Cfg::TILE_R + offr, &m3, &bars[s], ti * W, y, z);
         if constexpr (Cfg::CHI)
           tma_load_3d(st + 2 * Cfg::TILE_C + 2 * Cfg::TILE_R + offr, &m4, &bars[s], ti * W, y, z);
+      }
+    }
+    if constexpr (FOLDED) {
+      // the tile's folded table rows |kz| = 0 .. N/2 at |ky| (rows past N/2 of
+      // the last box lie outside the table and arrive zero-filled, unread)
+      const int fy = fold_index(to, a.rad_n1);
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        tma_load_3d(st + 2 * Cfg::TILE_C + size_t(b) * Cfg::RBF * W * sizeof(C), &m2, &bars[s], ti * W * 2, fy,
+                    b * Cfg::RBF);
+        if constexpr (Cfg::CHI)
+          tma_load_3d(st + 2 * Cfg::TILE_C + Cfg::FOLD_C + size_t(b) * Cfg::RBF * W * sizeof(Real), &m3, &bars[s],
+                      ti * W, fy, b * Cfg::RBF);
       }
     }
   };
@@ -214,7 +247,7 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
     }
     unsigned char *st = stage0 + s * Cfg::STAGE;
     C *tin = reinterpret_cast<C *>(st);
-    const int ti = t % sg.tiles_inner, to = t / sg.tiles_inner;
+    const int ti = t % sg.tiles_inner, to = outer(t / sg.tiles_inner);
     const long long base =
         sg.off + (long long)to * sg.s_outer + (long long)(ti * W + c) * sg.col_stride;
     const long long fs = sg.fft_stride;
@@ -260,6 +293,12 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
           if constexpr (Cfg::CHI) ch = rch[m];
         } else if constexpr (COMPUTED) {
           computed_ops<Real, MODEL>(a, ti * W + c, to, j + T * m, la, lb, ch);
+        } else if constexpr (FOLDED) {
+          const int fz = fold_index(j + T * m, N);
+          const C o = reinterpret_cast<const C *>(st + 2 * Cfg::TILE_C)[fz * W + c];
+          la = o.x;
+          lb = o.y;
+          if constexpr (Cfg::CHI) ch = reinterpret_cast<const Real *>(st + 2 * Cfg::TILE_C + Cfg::FOLD_C)[fz * W + c];
         } else {
           la = ta[e];
           lb = tb[e];
@@ -342,6 +381,8 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
             radial_ops(a, a.rad_M, cg, j + T * m, la, lb, ch);  // Nyquist plane: kx = M, ky = column
           } else if constexpr (COMPUTED) {
             computed_ops<Real, MODEL>(a, a.rad_M, cg, j + T * m, la, lb, ch);
+          } else if constexpr (FOLDED) {
+            folded_ops<Real, MODEL>(a, a.rad_M, cg, j + T * m, la, lb, ch);
           } else {
             la = a.tab_a[idx];
             lb = a.tab_b[idx];

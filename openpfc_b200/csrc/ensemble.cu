@@ -366,9 +366,14 @@ int opfc_ensemble_create(int count, const opfc_desc *descs, opfc_ensemble **out)
   if (cudaMemcpy(ep->d_inst, ep->inst.data(), sizeof(EnsInst) * count, cudaMemcpyHostToDevice) != cudaSuccess)
     return bail(OPFC_ERR_CUDA);
   // dynamic shared memory above 48 KB is never needed (N <= 128)
-  ep->var_col = AutoTuner::instance().get_config(ep->key + "/col", 0);
-  ep->var_x = AutoTuner::instance().get_config(ep->key + "/x", 0);
-  ep->var_upd = AutoTuner::instance().get_config(ep->key + "/upd", 0);
+  // cached choices come from a file: out-of-range entries fall back to variant 0
+  auto cached = [&](const char *stage) {
+    const int v = AutoTuner::instance().get_config(ep->key + stage, 0);
+    return (v >= 0 && v < kVariants) ? v : 0;
+  };
+  ep->var_col = cached("/col");
+  ep->var_x = cached("/x");
+  ep->var_upd = cached("/upd");
   *out = e.release();
   return OPFC_OK;
 }

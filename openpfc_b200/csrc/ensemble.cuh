@@ -307,13 +307,10 @@ template <typename Real, int W> constexpr size_t ens_x_smem() {
 // Persistent launch of kernel k: G CTAs per SM, or as many as fit (a CTA that
 // is not resident would hold its whole tile list back until a slot frees).
 template <typename K, typename... Args>
-int ens_persistent(K k, int G, int num_sms, int tiles, size_t smem, int threads, cudaStream_t s, int &occ,
-                   const Args &...args) {
-  if (!occ) {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess || occ < 1) occ = 1;
-    if (occ > G) occ = G;
-  }
+int ens_persistent(K k, int G, int num_sms, int tiles, size_t smem, int threads, cudaStream_t s,
+                   int (&setup)[kDevCache], const Args &...args) {
+  int occ = kernel_setup(k, threads, smem, setup);
+  if (occ > G) occ = G;
   const int grid = tiles < num_sms * occ ? tiles : num_sms * occ;
   if (grid < 1) return 0;
   k<<<grid, threads, smem, s>>>(args...);
@@ -324,20 +321,20 @@ template <typename Real, int W, int G>
 int ens_launch_stage_w(int stage, int num_sms, int tiles, int count, const EnsArgs &a, cudaStream_t s) {
   constexpr int NT = W * kEnsT;
   if (stage == 0) {
-    static int occ = 0;
+    static int setup[kDevCache];
     return ens_persistent(ens_col_kernel<Real, W, COL_PLAIN, +1, G>, G, num_sms, tiles, ens_col_smem<Real, W>(),
-                          NT, s, occ, a, 1);
+                          NT, s, setup, a, 1);
   } else if (stage == 2) {
-    static int occ = 0;
+    static int setup[kDevCache];
     return ens_persistent(ens_col_kernel<Real, W, COL_PLAIN, -1, G>, G, num_sms, tiles, ens_col_smem<Real, W>(),
-                          NT, s, occ, a, 1);
+                          NT, s, setup, a, 1);
   } else if (stage == 3) {
-    static int occ = 0;
+    static int setup[kDevCache];
     return ens_persistent(ens_col_kernel<Real, W, COL_UPDATE, -1, G>, G, num_sms, tiles,
-                          ens_col_smem<Real, W, COL_UPDATE>(), NT, s, occ, a, 2);
+                          ens_col_smem<Real, W, COL_UPDATE>(), NT, s, setup, a, 2);
   } else if (stage == 1) {
-    static int occ = 0;
-    return ens_persistent(ens_x_kernel<Real, W, G>, G, num_sms, tiles, ens_x_smem<Real, W>(), NT, s, occ, a);
+    static int setup[kDevCache];
+    return ens_persistent(ens_x_kernel<Real, W, G>, G, num_sms, tiles, ens_x_smem<Real, W>(), NT, s, setup, a);
   } else {
     ens_herm_kernel<Real><<<dim3(8, count), 256, 0, s>>>(a);
   }

@@ -1,7 +1,10 @@
 // io.cu -- on-disk formats of the reference's writers and readers (host code;
 // see io.h for the format rules and the reference files they follow).
+#include <fcntl.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <sys/types.h>
+#include <unistd.h>
 #include <string.h>
 
 #include <string>
@@ -75,31 +78,65 @@ int format_with_number(const char *pattern, int increment, std::string &out, std
   return OPFC_OK;
 }
 
+namespace {
+// pwrite all of `bytes` at `at`
+bool pwrite_all(int fd, const void *p, size_t bytes, off_t at) {
+  const char *c = static_cast<const char *>(p);
+  while (bytes) {
+    const ssize_t w = pwrite(fd, c, bytes, at);
+    if (w <= 0) return false;
+    c += w;
+    bytes -= (size_t)w;
+    at += w;
+  }
+  return true;
+}
+}  // namespace
+
 int write_box(const std::string &fn, const int global[3], const int local[3], const int offset[3],
               const double *data, int ncomp, std::string &err) {
-  FILE *f = fopen(fn.c_str(), "wb");  // truncates, like MPI_File_set_size(fh, 0)
-  if (!f) {
+  // The whole array truncates the file first (the reference's collective
+  // MPI_File_set_size(fh, 0) before MPI_File_write_all).  A smaller box is
+  // written in place, creating the file if it is missing but never truncating
+  // it, so several writers can each fill their own box of one file; the
+  // coordinator truncates and sizes the file once beforehand (prepare_box_file).
+  const bool whole = local[0] == global[0] && local[1] == global[1] && local[2] == global[2];
+  const int fd = open(fn.c_str(), O_WRONLY | O_CREAT | (whole ? O_TRUNC : 0), 0666);
+  if (fd < 0) {
     err = "cannot open \"" + fn + "\" for writing";
     return OPFC_ERR_IO;
   }
   const size_t row = (size_t)local[0] * ncomp;
-  const bool whole = local[0] == global[0] && local[1] == global[1] && local[2] == global[2];
   bool ok = true;
   if (whole) {
-    const size_t total = row * local[1] * local[2];
-    ok = fwrite(data, sizeof(double), total, f) == total;
+    ok = pwrite_all(fd, data, row * local[1] * local[2] * sizeof(double), 0);
   } else {
     for (int k = 0; k < local[2] && ok; ++k)
       for (int j = 0; j < local[1] && ok; ++j) {
         const long long at =
             ((long long)(offset[2] + k) * global[1] + (offset[1] + j)) * global[0] + offset[0];
-        ok = fseeko(f, (off_t)(at * ncomp * (long long)sizeof(double)), SEEK_SET) == 0 &&
-             fwrite(data + ((size_t)k * local[1] + j) * row, sizeof(double), row, f) == row;
+        ok = pwrite_all(fd, data + ((size_t)k * local[1] + j) * row, row * sizeof(double),
+                        (off_t)(at * ncomp * (long long)sizeof(double)));
       }
   }
-  ok = (fclose(f) == 0) && ok;
+  ok = (close(fd) == 0) && ok;
   if (!ok) {
     err = "short write to \"" + fn + "\"";
+    return OPFC_ERR_IO;
+  }
+  return OPFC_OK;
+}
+
+int prepare_box_file(const std::string &fn, const int global[3], int ncomp, std::string &err) {
+  const int fd = open(fn.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0666);
+  if (fd < 0) {
+    err = "cannot open \"" + fn + "\" for writing";
+    return OPFC_ERR_IO;
+  }
+  const off_t bytes = (off_t)global[0] * global[1] * global[2] * ncomp * (off_t)sizeof(double);
+  const bool ok = ftruncate(fd, bytes) == 0;
+  if (close(fd) != 0 || !ok) {
+    err = "cannot size \"" + fn + "\"";
     return OPFC_ERR_IO;
   }
   return OPFC_OK;
@@ -189,6 +226,13 @@ extern "C" int opfc_write_raw(const char *filename, const int global[3], const i
   if (!filename || !data || (ncomp != 1 && ncomp != 2) || !box_ok(global, local, offset)) return OPFC_ERR_ARG;
   std::string err;
   return opfc::io::write_box(filename, global, local, offset, data, ncomp, err);
+}
+
+extern "C" int opfc_prepare_raw(const char *filename, const int global[3], int ncomp) {
+  const int origin[3] = {0, 0, 0};
+  if (!filename || (ncomp != 1 && ncomp != 2) || !box_ok(global, global, origin)) return OPFC_ERR_ARG;
+  std::string err;
+  return opfc::io::prepare_box_file(filename, global, ncomp, err);
 }
 
 extern "C" int opfc_read_raw(const char *filename, const int global[3], const int local[3], const int offset[3],

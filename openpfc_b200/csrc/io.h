@@ -24,9 +24,14 @@ int format_with_number(const char *pattern, int increment, std::string &out, std
 
 // Write / read `count` doubles of the box `local` at `offset` of the global
 // array `global` (x fastest).  OPFC_ERR_IO on a file error, OPFC_ERR_SIZE when a
-// read finds fewer bytes than the box needs.
+// read finds fewer bytes than the box needs.  A write of the whole array
+// truncates the file first; a smaller box is written in place (the file is
+// created if missing, never truncated), so several writers can fill one file.
 int write_box(const std::string &fn, const int global[3], const int local[3], const int offset[3],
               const double *data, int ncomp, std::string &err);
+// Truncate `fn` and size it to the whole global array (zeros): done once by a
+// coordinator before several writers each write their box.
+int prepare_box_file(const std::string &fn, const int global[3], int ncomp, std::string &err);
 int read_box(const std::string &fn, const int global[3], const int local[3], const int offset[3], double *data,
              int ncomp, std::string &err);
 

@@ -39,10 +39,34 @@ template <typename Real> struct ColArgs {
   int rad_M, rad_n1, rad_n2;
   // computed operators: wavenumber steps, r, dt, 1/(2 alpha^2)
   Real kf0, kf1, kf2, op_r, op_dt, op_chi;
+  // folded tables: (opL, opN) pairs and the filter of the modes (kx, |ky|, |kz|),
+  // kx in [0, M], folded |ky| <= N1/2 and |kz| <= N2/2, in the split layout of an
+  // (M+1) x (N1/2+1) x (N2/2+1) grid (kx < M first, the kx = M plane at fold_nyq)
+  const void *fold_ops;
+  const Real *fold_chi;
+  long long fold_nyq;
 };
 
 // Operator selection of the fused z update.
-enum OpsKind { OPS_TABLES = 0, OPS_RADIAL = 1, OPS_COMPUTED = 2 };
+enum OpsKind { OPS_TABLES = 0, OPS_RADIAL = 1, OPS_COMPUTED = 2, OPS_FOLDED = 3 };
+
+// |k| index of a frequency index i of an axis of length n (i and n - i give
+// the same k^2, so every operator of k^2 is even in it)
+__device__ __forceinline__ int fold_index(int i, int n) { return i <= n / 2 ? i : n - i; }
+
+// Operators of mode (kx, ky, kz) read from the folded tables (direct loads).
+template <typename Real, int MODEL>
+__device__ __forceinline__ void folded_ops(const ColArgs<Real> &a, int kx, int ky, int kz, Real &la, Real &lb,
+                                           Real &ch) {
+  using C = typename Cx<Real>::T;
+  const long long r =
+      (long long)fold_index(ky, a.rad_n1) + (long long)(a.rad_n1 / 2 + 1) * fold_index(kz, a.rad_n2);
+  const long long i = kx < a.rad_M ? kx + (long long)a.rad_M * r : a.fold_nyq + r;
+  const C o = __ldg(reinterpret_cast<const C *>(a.fold_ops) + i);
+  la = o.x;
+  lb = o.y;
+  ch = MODEL != MK_PLAIN ? __ldg(a.fold_chi + i) : Real(1);
+}
 
 // Plain-PFC operators of mode (kx, ky, kz) (kx unfolded, ky / kz folded), in
 // the compute precision (10_complete_pfc_model.cpp:189-207, kspace.hpp:97-103):
@@ -158,6 +182,8 @@ __global__ void __launch_bounds__(Width<Real>::W *(N / EE)) col_kernel(const Col
           if constexpr (OPS == OPS_COMPUTED) {
             // z pass: main plane kx = column, ky = outer; Nyquist plane kx = M, ky = column
             computed_ops<Real, MODEL>(a, second ? a.rad_M : cg, second ? cg : to, j + T * m, la, lb, ch);
+          } else if constexpr (OPS == OPS_FOLDED) {
+            folded_ops<Real, MODEL>(a, second ? a.rad_M : cg, second ? cg : to, j + T * m, la, lb, ch);
           } else {
             la = a.tab_a[idx];
             lb = a.tab_b[idx];
@@ -659,6 +685,9 @@ template <typename Real> static ColArgs<Real> col_args(const ColLaunch &L) {
   a.op_r = (Real)L.op_r;
   a.op_dt = (Real)L.op_dt;
   a.op_chi = (Real)L.op_chi;
+  a.fold_ops = L.fold_ops;
+  a.fold_chi = reinterpret_cast<const Real *>(L.fold_chi);
+  a.fold_nyq = L.fold_nyq;
   return a;
 }
 
@@ -669,11 +698,8 @@ static int launch_col_direct(const ColLaunch &L, cudaStream_t s) {
   constexpr int NT = W * (N / EE);
   const size_t smem = sizeof(C) * ((size_t)N + (size_t)N * (W + 1));
   auto k = col_kernel<Real, N, MODE, DIR, MODEL, INV, OPS, EE>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  static int setup[kDevCache];
+  kernel_setup(k, NT, smem, setup);
   ColArgs<Real> a = col_args<Real>(L);
   const int tiles = a.seg0.ntiles + a.seg1.ntiles;
   if (tiles == 0) return 0;
@@ -692,18 +718,14 @@ static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
   using Cfg = TmaCfg<Real, N, W, MODE, MODEL, OPS, 3, PP>;
   constexpr int MINB = (NARROW && MODE == COL_PLAIN && 2 * (Cfg::SMEM + 1024) <= 233472 && NT <= 512) ? 2 : 1;
   if constexpr (Cfg::STAGES < 1 || (NARROW && MINB < 2) ||
-                (OPS == OPS_COMPUTED && MODEL == MK_TUNGSTEN)) {
+                (OPS == OPS_COMPUTED && MODEL == MK_TUNGSTEN) || (OPS == OPS_FOLDED && N % 16 != 0)) {
     return -1;
   } else {
     if (L.seg[0].ncols % W != 0 || L.seg[0].col_stride != 1) return -1;
     auto k = col_tma_kernel<Real, N, W, MODE, DIR, MODEL, INV, OPS, MINB, PP>;
-    static int occ = 0;
-    if (!occ) {
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, NT, Cfg::SMEM) != cudaSuccess || occ < 1)
-        occ = 1;
-      if (occ > MINB) occ = MINB;
-    }
+    static int setup[kDevCache];
+    int occ = kernel_setup(k, NT, Cfg::SMEM, setup);
+    if (occ > MINB) occ = MINB;
     ColArgs<Real> a = col_args<Real>(L);
     a.seg0 = retile(L.seg[0], W, Width<Real>::W);
     a.seg1 = L.nseg < 2 ? ColSeg{} : retile(L.seg[1], W, Width<Real>::W);
@@ -727,6 +749,8 @@ static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
       rc = L.rad_ops    ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_RADIAL, false>(L, s)
            : L.computed ? (L.pingpong ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false, true>(L, s)
                                       : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED, false>(L, s))
+           : L.fold_ops ? (L.pingpong ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_FOLDED, false, true>(L, s)
+                                      : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_FOLDED, false>(L, s))
                         : launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, false>(L, s);
     else
       rc = L.narrow     ? launch_col_tma<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, true>(L, s)
@@ -739,6 +763,9 @@ static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
   constexpr bool E32 = (N == 512 || N == 1024);
   if constexpr (MODE == COL_UPDATE && MODEL != MK_TUNGSTEN) {
     if (L.computed) return launch_col_direct<Real, N, MODE, DIR, MODEL, INV, OPS_COMPUTED>(L, s);
+  }
+  if constexpr (MODE == COL_UPDATE && MODEL != MK_ALUMINUM_G) {
+    if (L.fold_ops) return launch_col_direct<Real, N, MODE, DIR, MODEL, INV, OPS_FOLDED>(L, s);
   }
   if constexpr (MODE == COL_PLAIN && E32)
     if (L.e32) return launch_col_direct<Real, N, MODE, DIR, MODEL, INV, OPS_TABLES, 32>(L, s);
@@ -799,12 +826,8 @@ static int launch_x_sq(const XLaunch &L, cudaStream_t s) {
   if (L.rows % Cfg::W != 0 || Cfg::SMEM > (size_t)kMaxDynSmem) return -1;
   constexpr int NT = Cfg::W * R;
   auto k = x_sq_kernel<Real, R, MODEL, H>;
-  static int occ = 0;
-  if (!occ) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, NT, Cfg::SMEM) != cudaSuccess || occ < 1)
-      occ = 1;
-  }
+  static int setup[kDevCache];
+  const int occ = kernel_setup(k, NT, Cfg::SMEM, setup);
   const int ntiles = L.rows / Cfg::W;
   int G = (L.num_sms > 0 ? L.num_sms : 148) * occ;
   if (G > ntiles) G = ntiles;
@@ -817,12 +840,8 @@ static int launch_x_sqd(const XLaunch &L, cudaStream_t s) {
   using Cfg = XSqdCfg<Real, R, MODEL, H>;
   if (L.rows % Cfg::ROWS != 0 || Cfg::SMEM > (size_t)kMaxDynSmem) return -1;
   auto k = x_sqd_kernel<Real, R, MODEL, H>;
-  static int occ = 0;
-  if (!occ) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, Cfg::NT, Cfg::SMEM) != cudaSuccess || occ < 1)
-      occ = 1;
-  }
+  static int setup[kDevCache];
+  const int occ = kernel_setup(k, Cfg::NT, Cfg::SMEM, setup);
   const int ngroups = L.rows / Cfg::ROWS;
   int G = (L.num_sms > 0 ? L.num_sms : 148) * occ;
   if (G > ngroups) G = ngroups;
@@ -839,12 +858,8 @@ static int launch_x_tma(const XLaunch &L, cudaStream_t s) {
     if (L.rows % Cfg::W != 0 || Cfg::SMEM > (size_t)kMaxDynSmem) return -1;
     constexpr int NT = Cfg::W * (M / Plan<M>::E);
     auto k = x_tma_kernel<Real, M, MODEL>;
-    static int occ = 0;
-    if (!occ) {
-      cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM);
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, NT, Cfg::SMEM) != cudaSuccess || occ < 1)
-        occ = 1;
-    }
+    static int setup[kDevCache];
+    const int occ = kernel_setup(k, NT, Cfg::SMEM, setup);
     XArgs<Real> a;
     a.in0 = L.in0;
     a.in1 = L.in1;
@@ -881,11 +896,8 @@ static int launch_x_t(const XLaunch &L, cudaStream_t s) {
   constexpr int NT = W * (M / Plan<M>::E);
   const size_t smem = sizeof(C) * ((size_t)2 * M + (size_t)(M + 1) * (W + 1));
   auto k = x_kernel<Real, M, MODE, MODEL>;
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    attr = true;
-  }
+  static int setup[kDevCache];
+  kernel_setup(k, NT, smem, setup);
   XArgs<Real> a;
   a.in0 = L.in0;
   a.in1 = L.in1;

@@ -67,6 +67,13 @@ struct ColLaunch {
   // op_chi = 1 / (2 alpha^2) of the filter (FILTERED).  Uses rad_M/n1/n2.
   int computed;
   double kf[3], op_r, op_dt, op_chi;
+  // COL_UPDATE: operators from the folded FP64-built tables (opL, opN pairs and
+  // the filter over kx in [0, M], |ky| <= N1/2, |kz| <= N2/2; split layout with
+  // the kx = M plane at fold_nyq), the z tiles walked in (ky, N1 - ky) pairs so
+  // a table row is read from HBM once per step.  Uses rad_M/n1/n2.
+  const void *fold_ops;
+  const void *fold_chi;
+  long long fold_nyq;
   // COL_PLAIN: half-width tiles (64-byte rows) with two CTAs per SM
   int narrow;
   // ping-pong FFT exchange buffers (one CTA barrier per exchange; one ring
@@ -84,6 +91,7 @@ struct ColLaunch {
 // transforms (64-byte rows and half the tile for the narrow variant) and 64-byte
 // rows for the fused update (which stages psi_hat and the tables too), capped so
 // one tile stays near 64 KB / 32 KB.  Host and device use this one definition.
+// The folded-table update stages its table rows as 3 TMA boxes of N/4 rows.
 constexpr int tma_col_width(int N, int csize, int mode, bool narrow = false) {
   int w = (mode == COL_PLAIN && !narrow ? 128 : 64) / csize;
   const int cap = (mode == COL_PLAIN && !narrow ? 65536 : 32768) / (N * csize);
@@ -122,6 +130,34 @@ struct XLaunch {
   int sq_direct;       // X_FUSED: warp-square kernel with rows loaded straight into registers
   int num_sms;
 };
+
+// Per-device kernel set-up: the dynamic shared-memory attribute is a property
+// of the kernel on one device, so it is applied, and the resident CTAs per SM
+// are computed, once per device ordinal (cache[dev]); ordinals beyond the cache
+// are set up on every call.  Returns the resident CTAs per SM (>= 1).
+constexpr int kDevCache = 64;
+template <typename K> inline int kernel_setup(K k, int threads, size_t smem, int (&cache)[kDevCache]) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    dev = -1;
+  }
+  int *slot = (dev >= 0 && dev < kDevCache) ? &cache[dev] : nullptr;
+  if (slot && *slot) return *slot;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int occ = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, threads, smem) != cudaSuccess || occ < 1) {
+    cudaGetLastError();
+    occ = 1;
+  }
+  if (slot) *slot = occ;
+  return occ;
+}
+
+// The pass kernels' bounded mbarrier wait on a barrier that never completes,
+// with a limit of limit_ms (0.1 .. 1000): sets bit 2 of *flag when it expires
+// (wait_check.cu).  Returns cudaError_t as int.
+int launch_wait_check(unsigned *flag, double limit_ms, cudaStream_t s);
 
 // Kernel launchers (kernels_f32.cu / kernels_f64.cu).  Return cudaError_t as int.
 template <typename Real> int launch_col(const ColLaunch &a, cudaStream_t s);

@@ -1,11 +1,12 @@
 // noalloc.cu -- forward 3D R2C transform that allocates no device memory.
 //
-// Some callers cannot call cudaMalloc: code running while a CUDA graph is being
-// captured, allocation-free real-time loops, or hosts whose memory manager owns
-// every device allocation and forbids library-side allocations.  For them
-// opfc_fft_forward_noalloc runs the same passes as opfc_fft_forward (x R2C ->
-// y -> z -> reference layout) but keeps its intermediate half spectrum in the
-// file-scope device array below instead of a handle's work array.
+// Some callers cannot call cudaMalloc: latency-bound loops cannot absorb its
+// implicit device-wide synchronisation and unbounded run time, and some host
+// applications own every device allocation through their own memory manager
+// and do not let a library allocate.  For them opfc_fft_forward_noalloc runs the
+// same passes as opfc_fft_forward (x R2C -> y -> z -> reference layout) but
+// keeps its intermediate half spectrum in the file-scope device array below
+// instead of a handle's work array.
 //
 // The array is a fixed 16 MiB per GPU that loads the library and lives until the
 // process exits.  Every call shares it and it keeps the last call's contents;

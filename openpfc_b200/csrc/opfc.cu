@@ -37,7 +37,18 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 5, kVarX = 4, kVarZ = 6;
+constexpr int kVarY = 5, kVarX = 4, kVarZ = 9;
+// z-update variants by how they obtain opL / opN
+inline bool z_computed(int v) { return v >= 3 && v <= 5; }  // from k^2 in the compute precision
+inline bool z_folded(int v) { return v >= 6 && v <= 8; }    // folded FP64-built tables
+inline bool z_direct(int v) { return v == 2 || v == 4 || v == 7; }
+// OPFC_FP32_COMPUTED_OPERATORS=1 lets FP32 handles use (and tune) the update
+// variants that compute opL / opN per mode in FP32 (expm1f, fast divide)
+// instead of reading FP64-built tables rounded to FP32.
+inline bool computed_ops_allowed() {
+  const char *e = std::getenv("OPFC_FP32_COMPUTED_OPERATORS");
+  return e && e[0] == '1';
+}
 // models with two real fields per step (psi and psi_MF): Tungsten, Aluminum
 inline bool two_field(int model) { return model == OPFC_MODEL_TUNGSTEN || model == OPFC_MODEL_ALUMINUM; }
 // operator tables supplied by the caller (opfc_set_operators), filtered-model passes
@@ -131,6 +142,10 @@ struct opfc_handle {
   void *tab_ar = nullptr, *tab_br = nullptr;
   // isotropic grids: (opL, opN) and the filter as functions of m = |k_index|^2
   void *rad_ops = nullptr, *rad_chi = nullptr;
+  // every grid: (opL, opN) pairs and the filter over (kx, |ky|, |kz|), the
+  // FP64-built per-mode tables folded by the evenness of k^2 in ky and kz
+  void *fold_ops = nullptr, *fold_chi = nullptr;
+  long long fold_nyq = 0;
   void *adj_c[2] = {nullptr, nullptr};
   void *adj_r[3] = {nullptr, nullptr, nullptr};
 
@@ -148,7 +163,9 @@ struct opfc_handle {
   // var_z: 0 pipelined with streamed tables, 1 pipelined with radial tables,
   //        2 direct with streamed tables, 3 pipelined with computed operators,
   //        4 direct with computed operators, 5 as 3 with ping-pong exchange
-  //        buffers (3-5: PLAIN and FILTERED)
+  //        buffers (3-5: PLAIN and FILTERED), 6 pipelined with the folded
+  //        tables and ping-pong exchange buffers, 7 direct with the folded
+  //        tables, 8 pipelined with the folded tables
   int var_y = 0, var_x = 0, var_z = 0;
   int num_sms = 148;
   struct Tmap {
@@ -359,6 +376,36 @@ const CUtensorMap *tmap_for(opfc_handle *h, const void *ptr, int axis, int W, bo
   return &h->tmaps.back().map;
 }
 
+// Tensor map of a folded table ((M+1) x (N1/2+1) x (N2/2+1) modes in the split
+// layout, main part [N2/2+1][N1/2+1][S*M], S = 2 for (opL, opN) pairs, 1 for the
+// filter), box = W columns x 1 x N2/4 rows of |kz| (3 boxes cover |kz| <= N2/2).
+const CUtensorMap *tmap_fold(opfc_handle *h, const void *ptr, int W, bool pairs) {
+  if (!ptr || h->n2 % 16 != 0) return nullptr;
+  const int axis = pairs ? 3 : 4;  // cache keys apart from the full arrays' maps
+  for (const auto &t : h->tmaps)
+    if (t.ptr == ptr && t.axis == axis && t.W == W) return &t.map;
+  EncodeTiledFn enc = encode_fn();
+  if (!enc || h->tmaps.size() == h->tmaps.capacity()) return nullptr;
+  const cuuint64_t es = h->rsz, S = pairs ? 2 : 1;
+  const cuuint64_t F1 = h->n1 / 2 + 1, F2 = h->n2 / 2 + 1;
+  cuuint64_t dims[3] = {S * (cuuint64_t)h->M, F1, F2};
+  cuuint64_t strides[2] = {S * h->M * es, S * h->M * F1 * es};
+  cuuint32_t box[3] = {(cuuint32_t)(S * W), 1u, (cuuint32_t)(h->n2 / 4)};
+  cuuint32_t estr[3] = {1, 1, 1};
+  opfc_handle::Tmap t{};
+  t.ptr = ptr;
+  t.axis = axis;
+  t.W = W;
+  t.real = pairs ? 0 : 1;
+  const CUresult r = enc(&t.map, es == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                         3, const_cast<void *>(ptr), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return nullptr;
+  h->tmaps.push_back(t);
+  return &h->tmaps.back().map;
+}
+
 XLaunch x_base(opfc_handle *h) {
   XLaunch L{};
   L.M = h->M;
@@ -518,9 +565,14 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.tab_b = h->tab_b;
     Z.tab_chi = h->tab_chi;
     Z.axis = 2;
-    // computed operators (variants 3, 4): PLAIN and FILTERED models
-    Z.computed = h->var_z >= 3 && !two_field(model) && !user_ops_model(model);
-    Z.pingpong = h->var_z == 5;
+    // computed operators (variants 3-5): PLAIN and FILTERED models
+    Z.computed = z_computed(h->var_z) && !two_field(model) && !user_ops_model(model);
+    Z.pingpong = h->var_z == 5 || h->var_z == 6;
+    if (z_folded(h->var_z) && h->fold_ops) {
+      Z.fold_ops = h->fold_ops;
+      Z.fold_chi = h->fold_chi;
+      Z.fold_nyq = h->fold_nyq;
+    }
     Z.rad_M = h->M;
     Z.rad_n1 = h->n1;
     Z.rad_n2 = h->n2;
@@ -530,11 +582,15 @@ int enqueue_step(opfc_handle *h, int only = -1) {
     Z.op_dt = h->dt;
     Z.op_chi = model == OPFC_MODEL_FILTERED ? 1.0 / (2.0 * h->desc.filter_alpha * h->desc.filter_alpha) : 0.0;
     const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE);
-    if (h->use_tma && !h->al_grad && h->var_z != 2 && h->var_z != 4 && Z.N > 1 && h->M % W == 0) {
+    if (h->use_tma && !h->al_grad && !z_direct(h->var_z) && Z.N > 1 && h->M % W == 0) {
       Z.tmap[0] = tmap_for(h, h->work_a, 2, W, false);
       Z.tmap[1] = tmap_for(h, h->psi_hat, 2, W, false);
       if (Z.computed) {
         if (!Z.tmap[1]) Z.tmap[0] = nullptr;
+      } else if (Z.fold_ops) {
+        Z.tmap[2] = tmap_fold(h, h->fold_ops, W, true);
+        Z.tmap[3] = h->fold_chi ? tmap_fold(h, h->fold_chi, W, false) : nullptr;
+        if (!Z.tmap[1] || !Z.tmap[2] || (h->fold_chi && !Z.tmap[3])) Z.tmap[0] = nullptr;
       } else if (h->rad_ops && h->var_z == 1) {
         // isotropic grid: operators from the L2-resident radial tables
         Z.rad_ops = h->rad_ops;
@@ -934,7 +990,8 @@ int opfc_destroy(opfc_handle *h) {
   for (void *p : h->seg)
     if (p) cudaFree(p);
   void *adj[] = {h->tab_ar,   h->tab_br,   h->adj_c[0], h->adj_c[1], h->adj_r[0], h->adj_r[1],
-                 h->adj_r[2], h->rad_ops,  h->rad_chi,  h->tab_p,    h->work_c,   h->time_dev};
+                 h->adj_r[2], h->rad_ops,  h->rad_chi,  h->tab_p,    h->work_c,   h->time_dev,
+                 h->fold_ops, h->fold_chi};
   for (void *p : adj)
     if (p) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -1060,47 +1117,77 @@ int opfc_initialize(opfc_handle *h, double dt) {
     ob = (opCk == 0.0) ? kLap * dt : (oa - 1.0) / opCk;
     oc = fMF;
   };
+  // operators of one mode from its wave-vector components (FP64, the
+  // reference's formulas): oa = opL / exp_Ldt, ob = opN / n_weight, oc = filter
+  auto mode_ops = [&](double kx_, double ky_, double kz_, double &oa, double &ob, double &oc) {
+    if (model == OPFC_MODEL_ALUMINUM) {
+      const double kLap = -((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_));
+      aluminum_mode(kLap, oa, ob, oc);
+    } else if (model == OPFC_MODEL_TUNGSTEN) {
+      // physics_for_mode (tungsten_spectral.hpp:83-104) + spectral_exp_coeffs
+      // (spectral_exp_coefficients.hpp:68-82) + n_weight (tungsten_etd_workspace.hpp:111-130)
+      const double kLap = -((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_));
+      const double fMF = std::exp(kLap / lambda2);
+      const double kv = std::sqrt(-kLap) - 1.0;
+      const double k2 = kv * kv;
+      const double g1 = (P.alpha_highOrd == 0)
+                            ? std::exp(-k2 / alpha2)
+                            : std::exp(-(k2 + rTol * std::pow(kv, P.alpha_highOrd)) / alpha2);
+      const double g2 = 1.0 - 1.0 / alpha2 * k2;
+      const double gf = (kv < 0.0) ? g1 : g2;
+      const double opCk = P.stabP + p2b - peak * gf + q2b * fMF;
+      const double L = kLap * opCk;
+      const double arg = L * dt;
+      const double phi1 = (std::fabs(L) < 1e-12) ? dt + 0.5 * L * dt * dt : std::expm1(arg) / L;
+      oa = std::exp(arg);
+      ob = kLap * phi1;
+      oc = fMF;
+    } else {
+      // 10_complete_pfc_model.cpp:189-207
+      const double k2 = kx_ * kx_ + ky_ * ky_ + kz_ * kz_;
+      const double k2_lap = -k2;
+      const double L = k2_lap * (r + (1.0 - k2) * (1.0 - k2));
+      const double eL = std::exp(L * dt);
+      oa = eL;
+      ob = (std::fabs(L) > 1e-14) ? (eL - 1.0) / L * k2_lap : dt * k2_lap;
+      oc = need_chi ? std::exp(-k2 / (2.0 * fa * fa)) : 1.0;
+    }
+  };
   std::vector<double> tp(h->al_grad ? h->nc : 0);
   parallel_for((long)n2 * n1, [&](long row) {
     const int ky = (int)(row % n1), kz = (int)(row / n1);
     for (int kx = 0; kx < H; ++kx) {
       const double kx_ = kc(kx, n0, f0), ky_ = kc(ky, n1, f1), kz_ = kc(kz, n2, f2);
       const size_t o = split_index(h, kx, ky, kz);
-      if (model == OPFC_MODEL_ALUMINUM) {
-        const double kLap = -((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_));
-        aluminum_mode(kLap, ta[o], tb[o], tc[o]);
-        if (h->al_grad) tp[o] = aluminum_peak(kLap);
-      } else if (model == OPFC_MODEL_TUNGSTEN) {
-        // physics_for_mode (tungsten_spectral.hpp:83-104) + spectral_exp_coeffs
-        // (spectral_exp_coefficients.hpp:68-82) + n_weight (tungsten_etd_workspace.hpp:111-130)
-        const double kLap = -((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_));
-        const double fMF = std::exp(kLap / lambda2);
-        const double kv = std::sqrt(-kLap) - 1.0;
-        const double k2 = kv * kv;
-        const double g1 = (P.alpha_highOrd == 0)
-                              ? std::exp(-k2 / alpha2)
-                              : std::exp(-(k2 + rTol * std::pow(kv, P.alpha_highOrd)) / alpha2);
-        const double g2 = 1.0 - 1.0 / alpha2 * k2;
-        const double gf = (kv < 0.0) ? g1 : g2;
-        const double opCk = P.stabP + p2b - peak * gf + q2b * fMF;
-        const double L = kLap * opCk;
-        const double arg = L * dt;
-        const double phi1 = (std::fabs(L) < 1e-12) ? dt + 0.5 * L * dt * dt : std::expm1(arg) / L;
-        ta[o] = std::exp(arg);
-        tb[o] = kLap * phi1;
-        tc[o] = fMF;
-      } else {
-        // 10_complete_pfc_model.cpp:189-207
-        const double k2 = kx_ * kx_ + ky_ * ky_ + kz_ * kz_;
-        const double k2_lap = -k2;
-        const double L = k2_lap * (r + (1.0 - k2) * (1.0 - k2));
-        const double eL = std::exp(L * dt);
-        ta[o] = eL;
-        tb[o] = (std::fabs(L) > 1e-14) ? (eL - 1.0) / L * k2_lap : dt * k2_lap;
-        if (need_chi) tc[o] = std::exp(-k2 / (2.0 * fa * fa));
-      }
+      double oc = 1.0;
+      mode_ops(kx_, ky_, kz_, ta[o], tb[o], oc);
+      if (need_chi) tc[o] = oc;
+      if (h->al_grad) tp[o] = aluminum_peak(-((kx_ * kx_) + (ky_ * ky_) + (kz_ * kz_)));
     }
   });
+  // Folded tables: every operator is a function of k^2, and ky, n1 - ky (kz,
+  // n2 - kz) give the same k^2 bit for bit ((i - n) f = -((n - i) f) exactly),
+  // so the (M+1) x (n1/2+1) x (n2/2+1) modes with folded indices hold every
+  // per-mode value; the z update reads them (pairs (opL, opN) and the filter)
+  // instead of the full tables.  Not for the moving-gradient Aluminum model
+  // (its P_F term stays per mode).
+  std::vector<double> fo, fc;
+  const int F1 = n1 / 2 + 1, F2 = n2 / 2 + 1;
+  const size_t nf = (size_t)H * F1 * F2;
+  if (!h->al_grad) {
+    fo.resize(2 * nf);
+    if (need_chi) fc.resize(nf);
+    h->fold_nyq = (long long)h->M * F1 * F2;
+    parallel_for((long)F2 * F1, [&](long row) {
+      const int fy = (int)(row % F1), fz = (int)(row / F1);
+      for (int kx = 0; kx < H; ++kx) {
+        const size_t o = kx < h->M ? (size_t)kx + (size_t)h->M * row : (size_t)h->fold_nyq + row;
+        double oc = 1.0;
+        mode_ops(kc(kx, n0, f0), fy * f1, fz * f2, fo[2 * o], fo[2 * o + 1], oc);
+        if (need_chi) fc[o] = oc;
+      }
+    });
+  }
   auto upload = [&](std::vector<double> &src, void **dst) -> int {
     if (!*dst) {
       int rc = dev_alloc(h, dst, h->nc * h->rsz);
@@ -1114,10 +1201,25 @@ int opfc_initialize(opfc_handle *h, double dt) {
     }
     return OPFC_OK;
   };
+  auto upload_n = [&](const std::vector<double> &src, void **dst) -> int {
+    if (*dst) cudaFree(*dst);
+    *dst = nullptr;
+    int rc2 = dev_alloc(h, dst, src.size() * h->rsz);
+    if (rc2) return rc2;
+    if (h->prec == OPFC_FP64) {
+      CUDA_TRY(h, cudaMemcpy(*dst, src.data(), src.size() * 8, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(src.begin(), src.end());
+      CUDA_TRY(h, cudaMemcpy(*dst, f.data(), f.size() * 4, cudaMemcpyHostToDevice));
+    }
+    return OPFC_OK;
+  };
   int rc;
   if ((rc = upload(ta, &h->tab_a))) return rc;
   if ((rc = upload(tb, &h->tab_b))) return rc;
   if (need_chi && (rc = upload(tc, &h->tab_chi))) return rc;
+  if (!fo.empty() && (rc = upload_n(fo, &h->fold_ops))) return rc;
+  if (!fc.empty() && (rc = upload_n(fc, &h->fold_chi))) return rc;
   if (h->al_grad) {
     if ((rc = upload(tp, &h->tab_p))) return rc;
     h->pf0 = aluminum_peak(0.0);
@@ -1190,13 +1292,16 @@ static int finish_initialize(opfc_handle *h) {
   h->var_y = AutoTuner::instance().get_config(tune_key(h, "y"), 0);
   h->var_x = AutoTuner::instance().get_config(tune_key(h, "x"), 0);
   h->var_z = AutoTuner::instance().get_config(tune_key(h, "z"), 0);
+  // a cached FP32 choice with per-mode FP32 operators needs the opt-in
+  if (z_computed(h->var_z) && h->prec == OPFC_FP32 && !computed_ops_allowed()) h->var_z = h->fold_ops ? 6 : 0;
   if (const char *zv = std::getenv("OPFC_Z_VARIANT")) h->var_z = std::atoi(zv);
   if (const char *yv = std::getenv("OPFC_Y_VARIANT")) h->var_y = std::atoi(yv);
   if (const char *xv = std::getenv("OPFC_X_VARIANT")) h->var_x = std::atoi(xv);
   if (h->var_x < 0 || h->var_x >= kVarX) h->var_x = 0;
-  if (h->var_z == 1 && !h->rad_ops) h->var_z = 0;
-  if (h->var_z >= 3 && (two_field(model) || user_ops_model(model))) h->var_z = h->var_z == 4 ? 2 : 0;
   if (h->var_z < 0 || h->var_z >= kVarZ) h->var_z = 0;
+  if (h->var_z == 1 && !h->rad_ops) h->var_z = 0;
+  if (z_computed(h->var_z) && (two_field(model) || user_ops_model(model))) h->var_z = h->var_z == 4 ? 2 : 0;
+  if (z_folded(h->var_z) && !h->fold_ops) h->var_z = h->var_z == 7 ? 2 : 0;
   if (h->var_y < 0 || h->var_y >= kVarY) h->var_y = 0;
   h->initialized = true;
   h->a_valid = false;
@@ -1318,6 +1423,14 @@ int opfc_sync(opfc_handle *h) {
   return OPFC_OK;
 }
 
+int opfc_check_bounded_wait(opfc_handle *h, double limit_ms) {
+  if (!h) return OPFC_ERR_ARG;
+  if (!(limit_ms >= 0.1 && limit_ms <= 1000.0)) return fail(h, OPFC_ERR_ARG, "limit_ms must be in [0.1, 1000]");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  LAUNCH_TRY(h, launch_wait_check(h->flag, limit_ms, h->stream));
+  return OPFC_OK;
+}
+
 int opfc_fft_forward(opfc_handle *h, const void *in_real, void *out_complex, int dtype, int where) {
   if (!h || !in_real || !out_complex) return h ? fail(h, OPFC_ERR_ARG, "null pointer") : OPFC_ERR_ARG;
   int rc;
@@ -1430,7 +1543,11 @@ int opfc_autotune(opfc_handle *h, double *ms) {
       tune_key(h, "z"), kVarZ,
       [&](int v) {
         if (v == 1 && !h->rad_ops) return (int)OPFC_ERR_ARG;
-        if (v >= 3 && (two_field(h->desc.model) || user_ops_model(h->desc.model))) return (int)OPFC_ERR_ARG;
+        if (z_computed(v) && (two_field(h->desc.model) || user_ops_model(h->desc.model))) return (int)OPFC_ERR_ARG;
+        // FP32: operators computed in FP32 only when the caller opts in; the
+        // default keeps FP64-built tables rounded once to the compute precision
+        if (z_computed(v) && h->prec == OPFC_FP32 && !computed_ops_allowed()) return (int)OPFC_ERR_ARG;
+        if (z_folded(v) && !h->fold_ops) return (int)OPFC_ERR_ARG;
         h->var_z = v;
         return enqueue_step(h, 3);
       },
@@ -1570,6 +1687,30 @@ int opfc_ic_seeds(double *psi, const int n[3], const double dx[3], double n0, do
   return OPFC_OK;
 }
 
+// Rotation of a seed's wave vectors (seed.hpp rotate(), SeedFCC.hpp):
+// R = yaw(a0) (pitch(a1) roll(a2)), each matrix product and R q summed in index
+// order from zero, as the reference does, so the values agree bit for bit.
+static void rotate_q(const double ang[3], const double (*q0)[3], int nq, double (*out)[3]) {
+  const double ca = std::cos(ang[0]), sa = std::sin(ang[0]), cb = std::cos(ang[1]), sb = std::sin(ang[1]);
+  const double cc = std::cos(ang[2]), sc = std::sin(ang[2]);
+  const double Ra[3][3] = {{ca, -sa, 0}, {sa, ca, 0}, {0, 0, 1}};
+  const double Rb[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}};
+  const double Rc[3][3] = {{1, 0, 0}, {0, cc, -sc}, {0, sc, cc}};
+  double BC[3][3] = {}, R[3][3] = {};
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      for (int c = 0; c < 3; ++c) BC[a][b] += Rb[a][c] * Rc[c][b];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b)
+      for (int c = 0; c < 3; ++c) R[a][b] += Ra[a][c] * BC[c][b];
+  for (int v = 0; v < nq; ++v)
+    for (int a = 0; a < 3; ++a) {
+      double acc = 0;
+      for (int b = 0; b < 3; ++b) acc += R[a][b] * q0[v][b];
+      out[v][a] = acc;
+    }
+}
+
 // SeedGridFCC::apply (apps/aluminumNew/SeedGridFCC.hpp) with SeedFCC
 // (apps/aluminumNew/SeedFCC.hpp): one column of Ny x Nz seeds at x = X0 (Nx is
 // not used for placement), centres jittered by U(-0.2 r, 0.2 r) and Euler angles
@@ -1598,24 +1739,7 @@ int opfc_ic_seed_grid_fcc(double *psi, const int n[3], const double dx[3], const
       sd.c[2] = Dz / 2.0 + Dz * k + rt(re);
       double ang[3];
       for (double &a : ang) a = rr(re);
-      const double ca = std::cos(ang[0]), sa = std::sin(ang[0]), cb = std::cos(ang[1]), sb = std::sin(ang[1]);
-      const double cc = std::cos(ang[2]), sc = std::sin(ang[2]);
-      const double Ra[3][3] = {{ca, -sa, 0}, {sa, ca, 0}, {0, 0, 1}};
-      const double Rb[3][3] = {{cb, 0, sb}, {0, 1, 0}, {-sb, 0, cb}};
-      const double Rc[3][3] = {{1, 0, 0}, {0, cc, -sc}, {0, sc, cc}};
-      double BC[3][3] = {}, R[3][3] = {};
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b)
-          for (int c = 0; c < 3; ++c) BC[a][b] += Rb[a][c] * Rc[c][b];
-      for (int a = 0; a < 3; ++a)
-        for (int b = 0; b < 3; ++b)
-          for (int c = 0; c < 3; ++c) R[a][b] += Ra[a][c] * BC[c][b];
-      for (int v = 0; v < 4; ++v)
-        for (int a = 0; a < 3; ++a) {
-          double acc = 0;
-          for (int b = 0; b < 3; ++b) acc += R[a][b] * q0[v][b];
-          sd.q[v][a] = acc;
-        }
+      rotate_q(ang, q0, 4, sd.q);
       seeds.push_back(sd);
     }
   const double r2 = radius * radius;
@@ -1633,6 +1757,59 @@ int opfc_ic_seed_grid_fcc(double *psi, const int n[3], const double dx[3], const
           break;
         }
       }
+    }
+  });
+  return OPFC_OK;
+}
+
+// RandomSeeds::apply (include/openpfc/kernel/simulation/initial_conditions/
+// random_seeds.hpp:54-101) with Seed (seed.hpp): 150 seeds of radius 20 with
+// centres x ~ U(-108, -68), y, z ~ U(-128, 128) and Euler angles U(0, 2 pi),
+// drawn from std::mt19937_64(42) through std::uniform_real_distribution in the
+// reference's order (x, y, z, then the three angles, seed by seed).  Every cell
+// X = origin + i dx takes the value of the first seed that contains it,
+// rho + sum_q 2 amp cos(q . X) over the six rotated <110>/sqrt(2) vectors, and 0
+// outside every seed.
+int opfc_ic_random_seeds(double *psi, const int n[3], const double dx[3], const double origin[3], double density,
+                         double amplitude) {
+  if (!psi || !n || !dx || !origin || n[0] < 1 || n[1] < 1 || n[2] < 1) return OPFC_ERR_ARG;
+  constexpr int kSeeds = 150;
+  constexpr double kRadius = 20.0;
+  struct Seed {
+    double c[3], q[6][3];
+  };
+  std::mt19937_64 re(42);
+  std::uniform_real_distribution<double> rx(-128.0 + kRadius, -128.0 + 3 * kRadius);
+  std::uniform_real_distribution<double> ry(-128.0, 128.0);
+  std::uniform_real_distribution<double> rz(-128.0, 128.0);
+  std::uniform_real_distribution<double> ro(0.0, 8.0 * std::atan(1.0));
+  const double s = 1.0 / std::sqrt(2.0);
+  const double q0[6][3] = {{s, s, 0}, {s, 0, s}, {0, s, s}, {s, 0, -s}, {s, -s, 0}, {0, s, -s}};
+  std::vector<Seed> seeds(kSeeds);
+  for (Seed &sd : seeds) {
+    sd.c[0] = rx(re);
+    sd.c[1] = ry(re);
+    sd.c[2] = rz(re);
+    double ang[3];
+    for (double &a : ang) a = ro(re);
+    rotate_q(ang, q0, 6, sd.q);
+  }
+  const double r2 = kRadius * kRadius;
+  parallel_for((long)n[2] * n[1], [&](long row) {
+    const int j = (int)(row % n[1]), k = (int)(row / n[1]);
+    const double y = origin[1] + j * dx[1], z = origin[2] + k * dx[2];
+    for (int i = 0; i < n[0]; ++i) {
+      const double x = origin[0] + i * dx[0];
+      double u = 0.0;
+      for (const Seed &sd : seeds) {
+        const double ex = x - sd.c[0], ey = y - sd.c[1], ez = z - sd.c[2];
+        if (ex * ex + ey * ey + ez * ez < r2) {
+          u = density;
+          for (int v = 0; v < 6; ++v) u += 2.0 * amplitude * std::cos(sd.q[v][0] * x + sd.q[v][1] * y + sd.q[v][2] * z);
+          break;
+        }
+      }
+      psi[(size_t)row * n[0] + i] = u;
     }
   });
   return OPFC_OK;

@@ -22,11 +22,25 @@ _REF_OPS = os.path.join(_HERE, "_ref", "ref_ops")
 _lib = None
 
 
+# Where the reference source tree is mounted when this oracle is built next to
+# it; OPENPFC_REFERENCE_DIR overrides it.  Only the build recipe (make ref) and
+# the fixture generator read the tree; nothing on the GPU side needs it.
+_DEFAULT_REFERENCE_DIR = "/root/reference"
+
+
+def reference_dir():
+    """The reference source tree ($OPENPFC_REFERENCE_DIR, else the default
+    mount point), or None when it is absent."""
+    d = os.environ.get("OPENPFC_REFERENCE_DIR") or _DEFAULT_REFERENCE_DIR
+    return d if os.path.isdir(d) else None
+
+
 def build(ref: bool = True) -> None:
     """Compile liboracle.so (and _ref/ref_ops where the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", _HERE, "all"], check=True)
-    if ref and os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-C", _HERE, "ref"], check=True)
+    d = reference_dir()
+    if ref and d:
+        subprocess.run(["make", "-s", "-C", _HERE, "ref", f"REF={d}"], check=True)
 
 
 def lib():
@@ -55,6 +69,7 @@ def lib():
         L.orc_run_aluminum.argtypes = [ip, dp, dp, ctypes.c_void_p, cd, cd, cd, dp, ctypes.c_int, dp]
         L.orc_ic_seed_grid_fcc.argtypes = [dp, ip, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, cd, cd, cd,
                                            cd, cd]
+        L.orc_ic_random_seeds.argtypes = [dp, ip, dp, dp, cd, cd]
         L.orc_sum.argtypes = [dp, ctypes.c_size_t]
         L.orc_sum.restype = ctypes.c_double
         L.orc_free_energy_plain.argtypes = [ip, dp, ctypes.c_double, dp]
@@ -281,6 +296,14 @@ def ic_seed_grid_fcc(psi, dx, origin, Nx, Ny, Nz, X0, radius, amplitude, rho, rs
     return psi
 
 
+def ic_random_seeds(n, dx, origin, density, amplitude):
+    """RandomSeeds::apply (random_seeds.hpp:54-101): 150 rotated BCC seeds from
+    mt19937_64(42), 0 outside them; returns a (N2, N1, N0) field."""
+    psi = np.zeros((n[2], n[1], n[0]))
+    lib().orc_ic_random_seeds(_dp(psi), _ivec(n), _dvec(dx), _dvec(origin), float(density), float(amplitude))
+    return psi
+
+
 def run_filtered(psi, dx, r, alpha, p2, p3, p4, dt, nsteps, norms=False):
     psi = np.ascontiguousarray(psi, dtype=np.float64).copy()
     n = (psi.shape[2], psi.shape[1], psi.shape[0])
@@ -338,6 +361,17 @@ def mt64_stream(seed: int, count: int) -> np.ndarray:
 # ----------------------------------------------------------------------------
 # the reference's own operator code (only where the reference tree exists)
 # ----------------------------------------------------------------------------
+
+_REF_SEEDS = os.path.join(_HERE, "_ref", "ref_seeds")
+
+
+def ref_random_seeds(n, dx, origin, density, amplitude, tmpdir):
+    """Run _ref/ref_seeds (the reference's Seed class compiled in place)."""
+    path = os.path.join(tmpdir, f"ref_seeds_{n[0]}_{n[1]}_{n[2]}.bin")
+    args = [str(int(v)) for v in n] + [repr(float(v)) for v in dx] + [repr(float(v)) for v in origin]
+    subprocess.run([_REF_SEEDS] + args + [repr(float(density)), repr(float(amplitude)), path], check=True)
+    return np.fromfile(path, dtype=np.float64).reshape(n[2], n[1], n[0])
+
 
 def ref_ops_available() -> bool:
     return os.path.exists(_REF_OPS)

@@ -7,6 +7,7 @@ import subprocess
 import pytest
 
 import openpfc_b200 as ob
+import numpy as np
 from openpfc_b200 import _lib
 
 
@@ -100,3 +101,15 @@ def test_seed_grid_fcc_matches_oracle(oracle):
     a = ob.ic_seed_grid_fcc(base, [0.7, 0.9, 1.1], [-2.0, 1.0, 0.5], 1, 3, 2, 6.0, 5.0, 0.3, -0.05, 7)
     b = oracle.ic_seed_grid_fcc(base, [0.7, 0.9, 1.1], [-2.0, 1.0, 0.5], 1, 3, 2, 6.0, 5.0, 0.3, -0.05, 7)
     np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.parametrize("key,case", [
+    ("n32", ((32, 32, 32), (8.0, 8.0, 8.0), (-128.0, -128.0, -128.0), 0.5, 0.2)),
+    ("n16", ((16, 16, 16), (16.0, 16.0, 16.0), (-128.0, -128.0, -128.0), 0.65, 0.15))])
+def test_random_seeds_matches_reference_fixture(oracle, golden_dir, key, case):
+    """The product's RandomSeeds equals the reference-Seed fixture and the
+    oracle bit for bit (the domains of test_ic_random_seeds.cpp)."""
+    n, dx, org, rho, amp = case
+    got = ob.ic_random_seeds(n, dx, org, rho, amp)
+    np.testing.assert_array_equal(got, np.load(os.path.join(golden_dir, "random_seeds.npz"))[key])
+    np.testing.assert_array_equal(got, oracle.ic_random_seeds(n, dx, org, rho, amp))

@@ -14,7 +14,8 @@ pytestmark = pytest.mark.gpu
 PI4 = [math.pi / 4] * 3
 
 
-@pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "pingpong", "e32"])
+@pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "pingpong", "e32",
+                        "folded", "folded_direct", "folded_nopp"])
 def path(request, monkeypatch):
     """tma: pipelined kernels streaming the per-mode tables (default);
     tma_radial: the z update reading radial operator tables (OPFC_Z_VARIANT=1,
@@ -28,7 +29,13 @@ def path(request, monkeypatch):
     z update (OPFC_Y_VARIANT=3, OPFC_Z_VARIANT=5), and the x pass's warp-square
     kernel with rows loaded straight into registers (OPFC_X_VARIANT=3);
     e32: direct-load y pass with 32 values per thread (OPFC_Y_VARIANT=4;
-    other lengths keep their plan).
+    other lengths keep their plan);
+    folded: the z update reading the folded FP64-built tables with ping-pong
+    exchange buffers, with the ping-pong y pass and the register-loaded x pass
+    (OPFC_Y_VARIANT=3, OPFC_X_VARIANT=3, OPFC_Z_VARIANT=6);
+    folded_direct: direct-load z update on the folded tables (OPFC_Z_VARIANT=7);
+    folded_nopp: pipelined z update on the folded tables without ping-pong
+    buffers (OPFC_Z_VARIANT=8).
     The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
@@ -51,6 +58,14 @@ def path(request, monkeypatch):
         monkeypatch.setenv("OPFC_X_VARIANT", "3")
     elif request.param == "e32":
         monkeypatch.setenv("OPFC_Y_VARIANT", "4")
+    elif request.param == "folded":
+        monkeypatch.setenv("OPFC_Y_VARIANT", "3")
+        monkeypatch.setenv("OPFC_X_VARIANT", "3")
+        monkeypatch.setenv("OPFC_Z_VARIANT", "6")
+    elif request.param == "folded_direct":
+        monkeypatch.setenv("OPFC_Z_VARIANT", "7")
+    elif request.param == "folded_nopp":
+        monkeypatch.setenv("OPFC_Z_VARIANT", "8")
     return request.param
 
 
@@ -107,6 +122,7 @@ def test_autotune_then_parity(oracle, tmp_path, monkeypatch):
     monkeypatch.setenv("OPENPFC_GPU_AUTOTUNE_CACHE_DIR", str(tmp_path))
     monkeypatch.delenv("OPENPFC_GPU_AUTOTUNE_MODE", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
+    monkeypatch.delenv("OPFC_FP32_COMPUTED_OPERATORS", raising=False)
     n = (64, 64, 64)
     psi0 = oracle.ic_noise(n, -0.285, 0.01, 21)
     ref = oracle.run_plain(psi0, PI4, -0.25, 0.5, 10)
@@ -114,7 +130,10 @@ def test_autotune_then_parity(oracle, tmp_path, monkeypatch):
     m.initialize(0.5)
     ms = m.autotune()
     assert ms["y.pipelined"] > 0 and ms["y.narrow"] > 0 and ms["z.tables"] > 0 and ms["z.radial"] > 0
-    assert ms["z.computed"] > 0 and ms["z.direct_computed"] > 0
+    assert ms["z.folded_pingpong"] > 0 and ms["z.direct_folded"] > 0 and ms["z.folded"] > 0
+    # FP32 operators computed per mode are candidates only on request
+    assert ms["z.computed"] == -1 and ms["z.direct_computed"] == -1 and ms["z.computed_pingpong"] == -1
+    assert m.variants()[2] not in (3, 4, 5)
     chosen = m.variants()
     m.set_psi(psi0)
     m.step(10)
@@ -134,3 +153,14 @@ def test_transforms(oracle, path):
     Xo = oracle.r2c(x)
     assert np.abs(X - Xo).max() <= 1e-12 * np.abs(Xo).max()
     assert np.abs(f.backward(Xo) - oracle.c2r(Xo, n[0])).max() <= 1e-12 * np.abs(x).max()
+
+
+def test_autotune_fp32_computed_operators_on_request(tmp_path, monkeypatch):
+    monkeypatch.setenv("OPENPFC_GPU_AUTOTUNE_CACHE_DIR", str(tmp_path))
+    monkeypatch.delenv("OPENPFC_GPU_AUTOTUNE_MODE", raising=False)
+    monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
+    monkeypatch.setenv("OPFC_FP32_COMPUTED_OPERATORS", "1")
+    m = ob.PfcB200((64, 64, 64), PI4, precision=ob.FP32)
+    m.initialize(0.5)
+    ms = m.autotune()
+    assert ms["z.computed"] > 0 and ms["z.direct_computed"] > 0 and ms["z.computed_pingpong"] > 0

@@ -53,6 +53,27 @@ def test_raw_box_round_trip(tmp_path):
                             ob._dp(a), 1) == -8
 
 
+def test_two_writers_fill_one_file(tmp_path):
+    """Two writers, each with half of the global box (split along z and, in a
+    second file, along x), fill one file whose contents equal the whole array;
+    a stale longer file is truncated by the one-time prepare."""
+    L = _lib.lib()
+    g = (6, 5, 4)
+    a = np.arange(np.prod(g), dtype=np.float64).reshape(g[::-1]) * 0.25 + 1
+    for name, boxes in (("z", [((6, 5, 2), (0, 0, 0)), ((6, 5, 2), (0, 0, 2))]),
+                        ("x", [((3, 5, 4), (3, 0, 0)), ((3, 5, 4), (0, 0, 0))])):
+        fn = str(tmp_path / f"half_{name}.bin").encode()
+        np.zeros(1000).tofile(fn.decode())  # stale, longer file under the same name
+        assert L.opfc_prepare_raw(fn, _i3(g), 1) == 0
+        for loc, off in boxes:  # later writers never truncate what earlier ones wrote
+            part = np.ascontiguousarray(a[off[2]:off[2] + loc[2], off[1]:off[1] + loc[1],
+                                          off[0]:off[0] + loc[0]])
+            assert L.opfc_write_raw(fn, _i3(g), _i3(loc), _i3(off), ob._dp(part), 1) == 0
+        got = np.fromfile(fn.decode(), dtype=np.float64)
+        assert got.size == a.size
+        np.testing.assert_array_equal(got.reshape(a.shape), a)
+
+
 def test_cpp_io_mirrors(tmp_path):
     src = os.path.join(ROOT, "tests", "cpp", "test_io.cpp")
     exe = str(tmp_path / "test_io")

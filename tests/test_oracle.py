@@ -14,6 +14,8 @@ import os
 import numpy as np
 import pytest
 
+from oracle.oracle import reference_dir as _reference_dir
+
 
 @pytest.mark.parametrize("shape", [(8, 8, 8), (10, 12, 16), (8, 5, 6), (32, 32, 32), (5, 3, 2),
                                    (1, 1, 8), (1, 1, 2), (6, 10, 48), (4, 4, 80)])
@@ -93,7 +95,7 @@ def test_tungsten_tables_match_reference(oracle, golden_dir):
         np.testing.assert_allclose(ops[k], g[k], rtol=1e-14, atol=1e-300, err_msg=k)
 
 
-@pytest.mark.skipif(not os.path.isdir("/root/reference"), reason="reference tree absent")
+@pytest.mark.skipif(_reference_dir() is None, reason="reference tree absent (OPENPFC_REFERENCE_DIR)")
 def test_tungsten_tables_match_reference_live(oracle, tmp_path):
     oracle.build(ref=True)
     n, dx, dt = (8, 10, 12), 0.9, 0.5
@@ -178,3 +180,34 @@ def test_aluminum_moving_gradient_conserves_mass(oracle):
     assert abs(out.mean() - psi.mean()) <= 1e-12
     base = oracle.run_aluminum(psi, [1.0] * 3, [0.0] * 3, oracle.AluminumParams.test_case(), 1e-2, 3)
     assert np.abs(out - base).max() > 1e-6  # the gradient terms act
+
+
+RANDOM_SEEDS_CASES = {
+    "n32": ((32, 32, 32), (8.0, 8.0, 8.0), (-128.0, -128.0, -128.0), 0.5, 0.2),
+    "n16": ((16, 16, 16), (16.0, 16.0, 16.0), (-128.0, -128.0, -128.0), 0.65, 0.15),
+}
+
+
+@pytest.mark.parametrize("key", list(RANDOM_SEEDS_CASES))
+def test_random_seeds_matches_reference_seed_class(oracle, golden_dir, key):
+    """RandomSeeds on the domains of test_ic_random_seeds.cpp: the oracle equals,
+    bit for bit, the field computed with the reference's own Seed class
+    (tests/golden/random_seeds.npz), and has the properties that test checks:
+    some cells inside seeds, values within density +- 12 amplitude (+0.1),
+    deterministic."""
+    n, dx, org, rho, amp = RANDOM_SEEDS_CASES[key]
+    g = np.load(os.path.join(golden_dir, "random_seeds.npz"))[key]
+    got = oracle.ic_random_seeds(n, dx, org, rho, amp)
+    np.testing.assert_array_equal(got, g)
+    inside = got[got != 0.0]
+    assert inside.size > 0
+    assert inside.min() >= rho - 12 * amp - 0.1 and inside.max() <= rho + 12 * amp + 0.1
+    np.testing.assert_array_equal(oracle.ic_random_seeds(n, dx, org, rho, amp), got)
+
+
+@pytest.mark.skipif(_reference_dir() is None, reason="reference tree absent (OPENPFC_REFERENCE_DIR)")
+def test_random_seeds_matches_reference_live(oracle, tmp_path):
+    oracle.build(ref=True)
+    n, dx, org = (24, 20, 18), (10.0, 12.0, 13.0), (-120.0, -110.0, -100.0)
+    np.testing.assert_array_equal(oracle.ic_random_seeds(n, dx, org, 0.3, 0.1),
+                                  oracle.ref_random_seeds(n, dx, org, 0.3, 0.1, str(tmp_path)))

@@ -1,11 +1,13 @@
 """The allocation-free forward transform (opfc_fft_forward_noalloc) against the
-handle-based opfc_fft_forward, through the C ABI.
+handle-based opfc_fft_forward and the FP64 oracle, through the C ABI.
 
-It exists for callers that cannot allocate device memory (graph capture,
-allocation-free loops, hosts that own every allocation): its scratch is a fixed
-16 MiB array inside the library, shared by all calls.  Two calls in a row must
-both match the handle path; sizes beyond the array are refused.  This file is
-collected last so a failure here never hides the other tests.
+It exists for callers that cannot allocate device memory: latency-bound loops
+that cannot absorb cudaMalloc's device-wide synchronisation, and host
+applications whose own allocator owns every device allocation.  Its scratch is
+a fixed 16 MiB array inside the library, shared by all calls.  Two calls in a
+row must both match the handle path and the oracle; sizes beyond the array are
+refused.  This file is collected last so a failure here never hides the other
+tests, and it passes alone in a fresh process as well as after them.
 """
 import ctypes
 
@@ -30,7 +32,7 @@ def _noalloc(x_dev, out_dev, n, prec):
 
 @pytest.mark.parametrize("prec", [ob.FP64, ob.FP32])
 @pytest.mark.parametrize("n", [(64, 48, 32), (128, 64, 64), (32, 32, 32)])
-def test_noalloc_matches_handle_path_twice(prec, n):
+def test_noalloc_matches_handle_path_twice(oracle, prec, n):
     import torch
     tdt = torch.float64 if prec == ob.FP64 else torch.float32
     f = ob.B200Fft(n, precision=prec)
@@ -48,6 +50,12 @@ def test_noalloc_matches_handle_path_twice(prec, n):
         ref = ref[..., 0] + 1j * ref[..., 1]
         err = np.abs(got - ref).max() / np.abs(ref).max()
         assert err <= TOL[prec], (call, err)
+        # and the FP64 oracle's transform of the same input (values as the
+        # device holds them)
+        xo = x_dev.cpu().numpy().astype(np.float64)
+        ora = oracle.r2c(xo)
+        err_o = np.abs(got - ora).max() / np.abs(ora).max()
+        assert err_o <= TOL[prec], (call, err_o)
 
 
 def test_noalloc_rejects_sizes_beyond_its_array():
