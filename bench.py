@@ -426,11 +426,12 @@ def run_filtered(args):
     import torch
     import openpfc_b200 as ob
     n = 1024 if args.n == 512 else args.n
+    shape = tuple(args.shape) if args.shape else (n, n, n)
     hbm, peak_kind = peaks()
     t0 = time.time()
-    psi0 = ob.ic_seeds((n, n, n), DX, -0.10, 0.001, 8, 20.0, 0.2, 11)
+    psi0 = ob.ic_seeds(shape, DX, -0.10, 0.001, 8, 20.0, 0.2, 11)
     t_ic = time.time() - t0
-    m = ob.FilteredB200((n, n, n), DX, r=-0.3, alpha=0.5, p2=-0.1, p3=-0.5, p4=0.3, precision=ob.FP32)
+    m = ob.FilteredB200(shape, DX, r=-0.3, alpha=0.5, p2=-0.1, p3=-0.5, p4=0.3, precision=ob.FP32)
     m.initialize(DT)
     tune = None if args.no_autotune else m.autotune()
     m.set_psi(psi0)
@@ -438,17 +439,22 @@ def run_filtered(args):
     stream = torch.cuda.ExternalStream(m.stream)
     with Clocks(0) as ck:
         ms, _ = timed_steps(m, args.steps, args.warmup, 1, stream, repeats=args.repeats)
-    cells = n ** 3
-    nc = (n // 2 + 1) * n * n
+    cells = shape[0] * shape[1] * shape[2]
+    nc = (shape[0] // 2 + 1) * shape[1] * shape[2]
     prof = m.profile_step(reps=max(2, args.profile_reps // 2))
+    var_z = m.variants()[2]
+    tab = {0: 3 * nc * 4, 2: 3 * nc * 4}.get(var_z, 0)
+    if var_z in (6, 7, 8):
+        tab = 3 * 4 * (shape[0] // 2 + 1) * (shape[1] // 2 + 1) * (shape[2] // 2 + 1)
     ab = {"y_inverse": 16 * nc, "x_fused": 16 * nc, "y_forward": 16 * nc,
-          "z_update": nc * 32 + z_table_bytes(m.variants()[2], n, 3, 4), "hermitian_fix": 4 * 2 * n * n * 8}
+          "z_update": nc * 32 + tab, "hermitian_fix": 4 * 2 * shape[1] * shape[2] * 8}
     passes = {k: {"ms": t, "gbs": ab[k] / (t / 1e3) / 1e9, "frac": ab[k] / (t / 1e3) / 1e9 / hbm}
               for k, t in prof.items()}
     line = {"metric": "Mcell-steps/s, filtered PFC 1024^3 FP32", "value": cells * args.steps / (ms / 1e3) / 1e6,
             "unit": "Mcell-steps/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"mean-field-filtered PFC {n}^3 FP32, 8 seeds", "ic_seconds": t_ic},
+            "config": {"workload": f"mean-field-filtered PFC {'x'.join(map(str, shape))} FP32, 8 seeds",
+                       "operators": operator_source(var_z), "ic_seconds": t_ic},
             "alg_bytes_per_step": sum(ab.values()), "passes": passes, "peak": hbm, "peak_kind": peak_kind,
             "clocks": ck.summary(), "autotune": {"variants_yxz": m.variants(), "ms": tune}}
     print(json.dumps(line), flush=True)
@@ -566,6 +572,54 @@ def run_dry(args):
     return 0
 
 
+def run_adjoint(args):
+    """Adjoint calibration at 128^3 FP32: target from r* = -0.22, n0* = -0.28
+    (seed 3, 200 steps); forward with snapshots every 20 steps and the hand-written
+    adjoint at r = -0.25, n0 = -0.285 (gradients w.r.t. r, n0 and psi0).  Timed
+    on the host clock around the synchronous API calls (forward_checkpointed,
+    adjoint), after one untimed run of both."""
+    import torch
+    import openpfc_b200 as ob
+    n = (128, 128, 128)
+    steps, K = 200, 20
+    mt = ob.PfcB200(n, DX, r=-0.22, precision=ob.FP64)
+    mt.initialize(DT)
+    mt.set_psi(ob.ic_noise(n, -0.28, 0.01, 3))
+    mt.step(steps)
+    target = mt.get_psi().astype(np.float32)
+    del mt
+    m = ob.PfcB200(n, DX, r=-0.25, precision=ob.FP32)
+    m.initialize(DT)
+    psi0 = ob.ic_noise(n, -0.285, 0.01, 3).astype(np.float32)
+    dev_target = torch.tensor(target, device="cuda")
+    out = torch.empty_like(dev_target)
+    times = []
+    for rep in range(1 + args.repeats):
+        m.set_psi(psi0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        m.forward_checkpointed(steps, K)
+        t1 = time.perf_counter()
+        m.get_psi(out)
+        g, gr, gn = m.adjoint(out - dev_target)
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        if rep:
+            times.append((t1 - t0, t2 - t1))
+    fwd = statistics.median(t[0] for t in times)
+    adj = statistics.median(t[1] for t in times)
+    cells = n[0] * n[1] * n[2]
+    line = {"metric": "adjoint Mcell-steps/s, 128^3 FP32 (200 steps, snapshots every 20)",
+            "value": cells * steps / adj / 1e6, "unit": "Mcell-steps/s", "n_gpus": 1, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic", "steps": steps, "checkpoint_every": K,
+            "forward_checkpointed_ms": 1e3 * fwd, "adjoint_ms": 1e3 * adj,
+            "adjoint_ms_per_step": 1e3 * adj / steps,
+            "note": "adjoint time includes re-running every segment's forward steps from its snapshot",
+            "grad_r": gr, "grad_n0": gn, "repeats": len(times)}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
     ap = argparse.ArgumentParser()
@@ -583,9 +637,12 @@ def main(argv=None):
     ap.add_argument("--profile-reps", type=int, default=10)
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the cached (or default) kernel variants instead of timing them first")
-    ap.add_argument("--workload", default="plain", choices=["plain", "filtered", "ensemble"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "filtered", "ensemble", "adjoint"],
                     help="plain: the measured 512^3 line; filtered: mean-field-filtered 1024^3 FP32; "
-                         "ensemble: 256 uneven members, 50 steps in one graph")
+                         "ensemble: 256 uneven members, 50 steps in one graph; adjoint: 128^3 FP32 "
+                         "calibration (200 steps, snapshots every 20)")
+    ap.add_argument("--shape", type=int, nargs=3, default=None, metavar=("N0", "N1", "N2"),
+                    help="filtered workload only: a non-cubic grid (for profiling one pass on a small case)")
     ap.add_argument("--dry-run", action="store_true",
                     help="launch the ranks and print the line without GPU work (gloo; for tests)")
     args = ap.parse_args(argv)
@@ -606,6 +663,8 @@ def main(argv=None):
         return run_filtered(args)
     if args.workload == "ensemble":
         return run_ensemble(args)
+    if args.workload == "adjoint":
+        return run_adjoint(args)
     return run_b200(args)
 
 

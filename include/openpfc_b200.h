@@ -170,6 +170,14 @@ int opfc_kernels_per_step(const opfc_handle *h);
 int opfc_profile_step(opfc_handle *h, int reps, double *ms, int max_kernels);
 /* Name of kernel k of the step ("y_inverse", "x_fused", ...). */
 const char *opfc_step_kernel_name(int k);
+/* NVTX range name of kernel k: the reference's profiling regions whose work the
+ * kernel does (OPENPFC_PROFILE "gradient/mean_field/...", "gradient/evolve/...",
+ * apps/tungsten/include/tungsten/cpu/tungsten_model.hpp:313-362), pass in
+ * brackets.  opfc_profile_step times each kernel inside its range; with
+ * OPFC_NVTX=1 in the environment at opfc_create, opfc_step runs eagerly (no
+ * CUDA graph) and encloses every kernel in its range and every step in "step",
+ * so an NVTX-aware profiler groups the work by the reference's regions. */
+const char *opfc_step_kernel_region(int k);
 
 /* Autotuner (replaces pfc::gpu::AutoTuner::tune_kernel,
  * include/openpfc/runtime/common/gpu_autotune.hpp:295-333, same environment
@@ -202,15 +210,19 @@ const char *opfc_step_kernel_name(int k);
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 
-/* Adjoint of the plain model (no counterpart in the reference, which has no
- * differentiation).  opfc_set_r changes r (PLAIN/FILTERED) and rebuilds the
- * tables.  opfc_forward_checkpointed advances n_steps from the current state,
- * keeping a device snapshot of psi_hat every K steps.  opfc_adjoint then takes
- * dLoss/dpsi_T (real field, count N0*N1*N2) and returns dLoss/dpsi_0 (same
- * dtype/location), dLoss/dr and dLoss/dn0 = sum(dLoss/dpsi_0), re-running each
- * K-step segment from its snapshot and stepping the adjoint
- *   lambda_n = F^-1[opL F lambda] + 3 psi_n^2 F^-1[opN F lambda]
- * backwards; the handle is left at the forward run's final state. */
+/* Adjoint of the step (no counterpart in the reference, which has no
+ * differentiation) for the plain, filtered, Tungsten and Aluminum (G_grid = 0)
+ * models and caller-supplied operators.  opfc_set_r changes r
+ * (PLAIN/FILTERED) and rebuilds the tables.  opfc_forward_checkpointed advances
+ * n_steps from the current state, keeping a device snapshot of psi_hat every K
+ * steps.  opfc_adjoint then takes dLoss/dpsi_T (real field, count N0*N1*N2)
+ * and returns dLoss/dpsi_0 (same dtype/location), dLoss/dr (NaN for the
+ * models without r) and dLoss/dn0 = sum(dLoss/dpsi_0), re-running each K-step
+ * segment from its snapshot and stepping the adjoint
+ *   lambda_n = A lambda + dN/du (B lambda) + C[dN/dv (B lambda)]
+ * backwards, A = F^-1 opL F, B = F^-1 opN F, C = F^-1 chi F (the mean-field
+ * filter; u = psi, v = C psi; N the model's nonlinearity); the handle is left
+ * at the forward run's final state. */
 /* Uneven-size ensembles (no counterpart in the reference, which runs one field
  * per MPI job): `count` independent plain-PFC fields, each with its own size
  * (N0/2 in {16,24,32,40,48,64}, N1, N2 in {16,32,48,64,80,96,128}), dx and r,

@@ -238,6 +238,24 @@ class _ModelBase(_Handle):
         _check(self._h, lib().opfc_autotune(self._h, ms))
         return dict(zip(names, list(ms)))
 
+    def forward_checkpointed(self, n_steps: int, K: int = 20):
+        """Advance n_steps, keeping a snapshot every K steps for :meth:`adjoint`."""
+        _check(self._h, lib().opfc_forward_checkpointed(self._h, int(n_steps), int(K)))
+
+    def adjoint(self, grad_psi_T, out=None):
+        """(dLoss/dpsi0, dLoss/dr, dLoss/dn0) for dLoss/dpsi_T = grad_psi_T; dLoss/dr
+        is NaN for models without r (Tungsten, Aluminum, caller-supplied operators)."""
+        if out is None:
+            out = np.zeros(self.shape, dtype=np.float64) if isinstance(grad_psi_T, np.ndarray) \
+                else grad_psi_T.new_zeros(grad_psi_T.shape)
+        gp, gc, gdt, gloc = _buf(grad_psi_T)
+        op, oc, odt, oloc = _buf(out)
+        if gc != self.size_inbox() or oc != gc or gdt != odt or gloc != oloc:
+            raise ValueError("gradient buffers must be N0*N1*N2 values of one dtype and location")
+        gr, gn = ctypes.c_double(), ctypes.c_double()
+        _check(self._h, lib().opfc_adjoint(self._h, gp, gdt, gloc, op, ctypes.byref(gr), ctypes.byref(gn)))
+        return out, gr.value, gn.value
+
     def variants(self) -> tuple:
         v = (ctypes.c_int * 3)()
         _check(self._h, lib().opfc_variants(self._h, v))
@@ -279,23 +297,6 @@ class PfcB200(_ModelBase):
         _check(self._h, lib().opfc_set_r(self._h, float(r)))
         self.desc.r = float(r)
 
-    def forward_checkpointed(self, n_steps: int, K: int = 20):
-        """Advance n_steps, keeping a snapshot every K steps for :meth:`adjoint`."""
-        _check(self._h, lib().opfc_forward_checkpointed(self._h, int(n_steps), int(K)))
-
-    def adjoint(self, grad_psi_T, out=None):
-        """(dLoss/dpsi0, dLoss/dr, dLoss/dn0) for dLoss/dpsi_T = grad_psi_T."""
-        if out is None:
-            out = np.zeros(self.shape, dtype=np.float64) if isinstance(grad_psi_T, np.ndarray) \
-                else grad_psi_T.new_zeros(grad_psi_T.shape)
-        gp, gc, gdt, gloc = _buf(grad_psi_T)
-        op, oc, odt, oloc = _buf(out)
-        if gc != self.size_inbox() or oc != gc or gdt != odt or gloc != oloc:
-            raise ValueError("gradient buffers must be N0*N1*N2 values of one dtype and location")
-        gr, gn = ctypes.c_double(), ctypes.c_double()
-        _check(self._h, lib().opfc_adjoint(self._h, gp, gdt, gloc, op, ctypes.byref(gr), ctypes.byref(gn)))
-        return out, gr.value, gn.value
-
 
 class FilteredB200(_ModelBase):
     """Mean-field-filtered PFC: psi_MF = F^-1[exp(-k^2/(2 alpha^2)) psi_hat],
@@ -308,6 +309,10 @@ class FilteredB200(_ModelBase):
         d.model = MODEL_FILTERED
         d.r, d.filter_alpha, d.p2, d.p3, d.p4 = float(r), float(alpha), float(p2), float(p3), float(p4)
         super().__init__(d)
+
+    def set_r(self, r: float):
+        _check(self._h, lib().opfc_set_r(self._h, float(r)))
+        self.desc.r = float(r)
 
 
 class TungstenB200(_ModelBase):

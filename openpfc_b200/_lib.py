@@ -112,6 +112,8 @@ def lib():
     L.opfc_profile_step.argtypes = [H, ci, ctypes.POINTER(cd), ci]
     L.opfc_step_kernel_name.argtypes = [ci]
     L.opfc_step_kernel_name.restype = ctypes.c_char_p
+    L.opfc_step_kernel_region.argtypes = [ci]
+    L.opfc_step_kernel_region.restype = ctypes.c_char_p
     dp, ip = ctypes.POINTER(cd), ctypes.POINTER(ci)
     L.opfc_ic_noise.argtypes = [dp, sz, cd, cd, ctypes.c_uint64]
     L.opfc_ic_seed.argtypes = [dp, ip, dp, dp, dp, cd, cd, cd, ci]

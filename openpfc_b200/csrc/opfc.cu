@@ -23,6 +23,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/openpfc_b200.h"
 #include "fft_core.cuh"
 #include "launch.h"
@@ -147,12 +149,15 @@ struct opfc_handle {
   void *fold_ops = nullptr, *fold_chi = nullptr;
   long long fold_nyq = 0;
   void *adj_c[2] = {nullptr, nullptr};
-  void *adj_r[3] = {nullptr, nullptr, nullptr};
+  void *adj_r[4] = {nullptr, nullptr, nullptr, nullptr};
 
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t graph_exec = nullptr;
 
   bool use_tma = true;  // TMA-fed column passes (OPFC_NO_TMA=1 disables)
+  // OPFC_NVTX=1: steps run eagerly (no CUDA graph) with one NVTX range per
+  // kernel named after the reference's profiling regions
+  bool nvtx = false;
   // kernel variants per pass, chosen by the autotuner (see opfc_autotune):
   // var_y: 0 pipelined, 1 direct, 2 pipelined narrow tiles (two CTAs per SM),
   //        3 pipelined with ping-pong exchange buffers, 4 direct with 32
@@ -474,9 +479,39 @@ int prepare_a(opfc_handle *h) {
 constexpr int kStepKernels = 5;
 const char *const kStepKernelNames[kStepKernels] = {"y_inverse", "x_fused", "y_forward",
                                                      "z_update", "hermitian_fix"};
+// NVTX range of each step kernel, named after the profiling regions of the
+// reference's step (OPENPFC_PROFILE, apps/tungsten/include/tungsten/cpu/
+// tungsten_model.hpp:313-362) whose work the kernel does, with the pass in brackets.
+const char *const kStepRegions[kStepKernels] = {
+    "gradient/mean_field/backward [y inverse]",
+    "gradient/mean_field/backward + nonlinear + gradient/evolve/forward [x: C2R, N, R2C]",
+    "gradient/evolve/forward [y forward]",
+    "gradient/evolve/forward + multiply + backward [z forward, ETD combine, z inverse]",
+    "gradient/evolve/multiply [Hermitian projection]"};
 
-// Enqueue the step's kernels on h->stream; `only` >= 0 enqueues that one kernel.
+// nvtxRangePushA / nvtxRangePop around a scope (a no-op without an NVTX tool)
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+};
+
+int enqueue_step_kernels(opfc_handle *h, int only);
+
+// Enqueue the step's kernels on h->stream; `only` >= 0 enqueues that one
+// kernel.  With NVTX ranges on (eager steps, opfc_profile_step) each kernel is
+// enqueued inside the range of its reference region.
 int enqueue_step(opfc_handle *h, int only = -1) {
+  if (!h->nvtx) return enqueue_step_kernels(h, only);
+  for (int k = 0; k < kStepKernels; ++k) {
+    if (only >= 0 && k != only) continue;
+    NvtxRange range(kStepRegions[k]);
+    const int rc = enqueue_step_kernels(h, k);
+    if (rc) return rc;
+  }
+  return OPFC_OK;
+}
+
+int enqueue_step_kernels(opfc_handle *h, int only) {
   const int model = h->desc.model;
   if (only < 0 || only == 0) {  // YI
     if (two_field(model)) {
@@ -990,8 +1025,8 @@ int opfc_destroy(opfc_handle *h) {
   for (void *p : h->seg)
     if (p) cudaFree(p);
   void *adj[] = {h->tab_ar,   h->tab_br,   h->adj_c[0], h->adj_c[1], h->adj_r[0], h->adj_r[1],
-                 h->adj_r[2], h->rad_ops,  h->rad_chi,  h->tab_p,    h->work_c,   h->time_dev,
-                 h->fold_ops, h->fold_chi};
+                 h->adj_r[2], h->adj_r[3], h->rad_ops,  h->rad_chi,  h->tab_p,    h->work_c,
+                 h->time_dev, h->fold_ops, h->fold_chi};
   for (void *p : adj)
     if (p) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -1025,6 +1060,8 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   {
     const char *no = std::getenv("OPFC_NO_TMA");
     h->use_tma = !(no && no[0] == '1');
+    const char *nv = std::getenv("OPFC_NVTX");
+    h->nvtx = nv && nv[0] == '1';
   }
   cudaError_t e = cudaSetDevice(h->device);
   if (e != cudaSuccess) return OPFC_ERR_CUDA;
@@ -1402,6 +1439,13 @@ int opfc_step(opfc_handle *h, int n_steps) {
   CUDA_TRY(h, cudaSetDevice(h->device));
   int rc;
   if (!h->a_valid && (rc = prepare_a(h))) return rc;
+  if (h->nvtx) {  // eager, one NVTX range per kernel
+    for (int s = 0; s < n_steps; ++s) {
+      NvtxRange range("step");
+      if ((rc = enqueue_step(h))) return rc;
+    }
+    return OPFC_OK;
+  }
   if (!h->graph_exec) {
     if ((rc = build_graph(h))) return rc;
   }
@@ -1585,10 +1629,12 @@ int opfc_profile_step(opfc_handle *h, int reps, double *ms, int max_kernels) {
   CUDA_TRY(h, cudaEventCreate(&e1));
   const int nk = std::min(max_kernels, kStepKernels);
   for (int k = 0; k < nk; ++k) {
-    // one untimed launch, then `reps` timed launches of kernel k alone
-    if ((rc = enqueue_step(h, k))) break;
+    // one untimed launch, then `reps` timed launches of kernel k alone, inside
+    // the NVTX range of its reference region
+    NvtxRange range(kStepRegions[k]);
+    if ((rc = enqueue_step_kernels(h, k))) break;
     cudaEventRecord(e0, h->stream);
-    for (int r = 0; r < reps && !rc; ++r) rc = enqueue_step(h, k);
+    for (int r = 0; r < reps && !rc; ++r) rc = enqueue_step_kernels(h, k);
     cudaEventRecord(e1, h->stream);
     cudaEventSynchronize(e1);
     float t = 0;
@@ -1819,42 +1865,84 @@ const char *opfc_step_kernel_name(int k) {
   return (k >= 0 && k < kStepKernels) ? kStepKernelNames[k] : "";
 }
 
+const char *opfc_step_kernel_region(int k) { return (k >= 0 && k < kStepKernels) ? kStepRegions[k] : ""; }
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
-// Adjoint of the plain conserved PFC step (checkpoint-and-recompute).
+// Adjoint of the PFC step (checkpoint-and-recompute) for the plain, filtered,
+// Tungsten and Aluminum (G_grid = 0) models and caller-supplied operators.
 //
-// In real space one step is psi' = A psi + B (psi^3) with A = F^-1 opL F and
-// B = F^-1 opN F (10_complete_pfc_model.cpp:121-144).  opL, opN are real and
-// even in k, so A and B are symmetric and the adjoint step is
-//   lambda_n = A lambda_{n+1} + 3 psi_n^2 (B lambda_{n+1}).
-// With opL = exp(L dt), L = -k^2 (r + (1-k^2)^2) and opN = dt (-k^2) phi(L dt),
-// phi(x) = (e^x - 1)/x, the parameter derivative is
+// In real space one step is psi' = A psi + B N(psi, C psi) with A = F^-1 opL F,
+// B = F^-1 opN F and the mean-field filter C = F^-1 chi F (C = 1 for the plain
+// model): N = psi^3 (10_complete_pfc_model.cpp:121-144); N = c0 v^2 + c1 v^3 +
+// c2 v^4 of v = C psi (filtered, caller-supplied operators); N = c0 u^2 +
+// c1 u^3 + c2 v^2 + c3 v^3 - c4 u of u = psi, v = C psi (Tungsten,
+// cpu/tungsten_model.hpp:334-350, tungsten_ops_kernels.cu:25-58; Aluminum
+// with G_grid = 0, Aluminum.hpp:285-307).  opL, opN and chi are real and even
+// in k, so A, B and C are symmetric and the adjoint step is
+//   lambda_n = A lambda_{n+1} + dN/du (B lambda_{n+1}) + C[dN/dv (B lambda_{n+1})]
+// (the conjugate spectral multiplies are the multiplies themselves, the
+// adjoint filter is the filter).  For the models with L = -k^2 (r + (1-k^2)^2)
+// (plain, filtered), opL = exp(L dt) and opN = dt (-k^2) phi(L dt) with
+// phi(x) = (e^x - 1)/x, so
 //   dLoss/dr = sum_n <lambda_{n+1}, F^-1[dopL/dr psi_hat_n + dopN/dr N_hat_n]>
 //            = sum_n (1/N) sum_k w_kx Re(conj(lambda_hat) (...)),
 // dopL/dr = -k^2 dt opL,  dopN/dr = dt^2 k^4 phi'(L dt),
-// accumulated in FP64.  psi_n comes from re-running the forward step (the same
-// CUDA graph) from the nearest snapshot.
+// accumulated in FP64 per reduction block on the device across all steps.
+// psi_n comes from re-running the forward step (the same CUDA graph) from the
+// nearest snapshot.
 // ---------------------------------------------------------------------------
 
+// Nonlinearity of the step's model from u = psi and v = C psi (in real space,
+// the mean included); `kind` 0 plain, 1 filtered, 2 Tungsten form.
 template <typename Real>
-__global__ void cube_kernel(const Real *x, Real *y, size_t n) {
+__global__ void adj_nonlin_kernel(const Real *u, const Real *v, Real *out, size_t n, int kind, double c0,
+                                  double c1, double c2, double c3, double c4) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const Real v = x[i];
-    y[i] = v * v * v;
+    const Real a = u[i];
+    Real r;
+    if (kind == 0) {
+      r = a * a * a;
+    } else if (kind == 1) {
+      const Real b = v[i];
+      r = b * b * (Real(c0) + Real(c1) * b + Real(c2) * b * b);
+    } else {
+      const Real b = v[i];
+      r = a * a * (Real(c0) + Real(c1) * a) + b * b * (Real(c2) + Real(c3) * b) - Real(c4) * a;
+    }
+    out[i] = r;
+  }
+}
+
+// lam += dN/du (u, v) w  and  g = dN/dv (u, v) w  (g unused for the plain model)
+template <typename Real>
+__global__ void adj_jacobian_kernel(const Real *u, const Real *v, const Real *w, Real *lam, Real *g, size_t n,
+                                    int kind, double c0, double c1, double c2, double c3, double c4) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const Real a = u[i], x = w[i];
+    if (kind == 0) {
+      lam[i] += Real(3) * a * a * x;  // d(psi^3)/dpsi
+    } else if (kind == 1) {
+      const Real b = v[i];  // d(c0 v^2 + c1 v^3 + c2 v^4)/dv
+      g[i] = b * (Real(2 * c0) + Real(3 * c1) * b + Real(4 * c2) * b * b) * x;
+    } else {
+      const Real b = v[i];
+      lam[i] += (a * (Real(2 * c0) + Real(3 * c1) * a) - Real(c4)) * x;  // dN/du
+      g[i] = b * (Real(2 * c2) + Real(3 * c3) * b) * x;                  // dN/dv
+    }
   }
 }
 
 template <typename Real>
-__global__ void adj_combine_kernel(const Real *u, const Real *psi, const Real *w, Real *lam, size_t n) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    const Real p = psi[i];
-    lam[i] = u[i] + Real(3) * p * p * w[i];
-  }
+__global__ void adj_add_kernel(Real *lam, const Real *x, size_t n) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    lam[i] += x[i];
 }
 
 // U = opL lam_hat (in place over lam_hat), V = opN lam_hat (over n_hat, after
-// it is read), and FP64 partial sums of w_kx Re(conj(lam_hat)(dA psi_hat + dB n_hat)).
+// it is read), and (tar != nullptr) FP64 sums of w_kx Re(conj(lam_hat)(dA psi_hat
+// + dB n_hat)) added to this block's running partial.
 template <typename Real>
 __global__ void adj_modes_kernel(typename opfc::Cx<Real>::T *lam_hat, const typename opfc::Cx<Real>::T *psi_hat,
                                  typename opfc::Cx<Real>::T *n_hat, const Real *ta, const Real *tb,
@@ -1866,26 +1954,29 @@ __global__ void adj_modes_kernel(typename opfc::Cx<Real>::T *lam_hat, const type
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nc;
        i += (long long)gridDim.x * blockDim.x) {
     const auto l = lam_hat[i];
-    const auto p = psi_hat[i];
-    const auto q = n_hat[i];
-    const double ar = tar[i], br = tbr[i];
-    const double gx = ar * p.x + br * q.x, gy = ar * p.y + br * q.y;
-    const int kx = i < nyq_off ? (int)(i % M) : M;
-    const double wgt = (kx == 0 || kx == M) ? 1.0 : 2.0;
-    s += wgt * ((double)l.x * gx + (double)l.y * gy);
+    if (tar) {
+      const auto p = psi_hat[i];
+      const auto q = n_hat[i];
+      const double ar = tar[i], br = tbr[i];
+      const double gx = ar * p.x + br * q.x, gy = ar * p.y + br * q.y;
+      const int kx = i < nyq_off ? (int)(i % M) : M;
+      const double wgt = (kx == 0 || kx == M) ? 1.0 : 2.0;
+      s += wgt * ((double)l.x * gx + (double)l.y * gy);
+    }
     const Real a = ta[i], b = tb[i];
     lam_hat[i].x = a * l.x;
     lam_hat[i].y = a * l.y;
     n_hat[i].x = b * l.x;
     n_hat[i].y = b * l.y;
   }
+  if (!tar) return;
   red[threadIdx.x] = s;
   __syncthreads();
   for (int hh = blockDim.x / 2; hh > 0; hh >>= 1) {
     if (threadIdx.x < hh) red[threadIdx.x] += red[threadIdx.x + hh];
     __syncthreads();
   }
-  if (threadIdx.x == 0) partials[blockIdx.x] = red[0];
+  if (threadIdx.x == 0) partials[blockIdx.x] += red[0];
 }
 
 namespace {
@@ -1923,7 +2014,43 @@ double dphi(double x) {
   return (x * std::exp(x) - std::expm1(x)) / (x * x);
 }
 
+// models whose operators depend on r (L = -k^2 (r + (1 - k^2)^2))
+bool has_r(const opfc_handle *h) {
+  return h->desc.model == OPFC_MODEL_PLAIN || h->desc.model == OPFC_MODEL_FILTERED;
+}
+
+// nonlinearity kind and coefficients of the adjoint kernels
+int adj_kind(const opfc_handle *h, double c[5]) {
+  const int model = h->desc.model;
+  for (int i = 0; i < 5; ++i) c[i] = 0.0;
+  if (model == OPFC_MODEL_PLAIN) return 0;
+  if (model == OPFC_MODEL_FILTERED || user_ops_model(model)) {
+    c[0] = h->desc.p2 / 2.0;
+    c[1] = h->desc.p3 / 3.0;
+    c[2] = h->desc.p4 / 4.0;
+    return 1;
+  }
+  if (model == OPFC_MODEL_ALUMINUM) {  // as the forward x pass (G_grid = 0)
+    const opfc_aluminum_params &p = h->desc.aluminum;
+    c[0] = p.p3_bar;
+    c[1] = p.p4_bar;
+    c[2] = p.q31_bar * p.T_const / p.T0 + p.q30_bar;
+    c[3] = p.q4_bar;
+    c[4] = p.stabP;
+    return 2;
+  }
+  const opfc_tungsten_params &p = h->desc.tungsten;  // tungsten_params.hpp:339-411
+  const double tau = p.T / p.T0;
+  c[0] = p.shift_u * (p.p3 + 3 * p.shift_s * p.p4);
+  c[1] = std::pow(p.shift_u, 2) * p.p4;
+  c[2] = p.shift_u * p.q31 * tau + p.shift_u * (p.q30 + 3.0 * p.shift_s * p.q40);
+  c[3] = std::pow(p.shift_u, 2) * p.q40;
+  c[4] = p.stabP;
+  return 2;
+}
+
 int adjoint_tables(opfc_handle *h) {
+  if (!has_r(h)) return OPFC_OK;  // no r-derivative tables
   const int n0 = h->n0, n1 = h->n1, n2 = h->n2, H = h->M + 1;
   const double f0 = 2.0 * kPi / (h->desc.dx[0] * n0);
   const double f1 = 2.0 * kPi / (h->desc.dx[1] * n1);
@@ -1978,50 +2105,71 @@ int adjoint_buffers(opfc_handle *h) {
   return OPFC_OK;
 }
 
-// lambda (adj_r[0]) <- adjoint of the step taken from psi_hat_n; adds the step's
-// dLoss/dr contribution to *dr.
-int adjoint_step(opfc_handle *h, const void *psi_hat_n, double *dr) {
-  void *lam = h->adj_r[0], *psi = h->adj_r[1], *tmp = h->adj_r[2];
+template <typename Real, typename K, typename... A> int elt(opfc_handle *h, K k, A... args) {
+  k<<<kEltBlocks, 256, 0, h->stream>>>(args...);
+  CUDA_TRY(h, cudaGetLastError());
+  return OPFC_OK;
+}
+
+// lambda (adj_r[0]) <- adjoint of the step taken from psi_hat_n; for the models
+// with r the step's dLoss/dr terms are added to the running per-block FP64
+// partials (h->partials, summed once at the end).
+int adjoint_step(opfc_handle *h, const void *psi_hat_n) {
+  void *lam = h->adj_r[0], *u = h->adj_r[1], *tmp = h->adj_r[2], *v = h->adj_r[3];
   void *c0 = h->adj_c[0], *c1 = h->adj_c[1];
   const bool f64 = h->prec == OPFC_FP64;
+  double cf[5];
+  const int kind = adj_kind(h, cf);
+  const double mean = mean_density(h);
   int rc;
-  // psi_n in real space, N_hat_n = F[psi_n^3]
+  // u = psi_n, v = C psi_n in real space; N_hat_n = F[N(u, v)]
   if ((rc = copy_state(h, c0, psi_hat_n))) return rc;
-  if ((rc = bwd_real(h, c0, psi, mean_density(h)))) return rc;
+  if ((rc = bwd_real(h, c0, u, mean))) return rc;
+  if (kind != 0) {
+    if ((rc = opfc_scale_by_table(h, psi_hat_n, h->tab_chi, c0))) return rc;
+    if ((rc = bwd_real(h, c0, v, mean))) return rc;  // chi(0) = 1: the mean passes the filter
+  }
   if (f64)
-    cube_kernel<double><<<kEltBlocks, 256, 0, h->stream>>>((const double *)psi, (double *)tmp, h->nr);
+    rc = elt<double>(h, adj_nonlin_kernel<double>, (const double *)u, (const double *)v, (double *)tmp, h->nr,
+                     kind, cf[0], cf[1], cf[2], cf[3], cf[4]);
   else
-    cube_kernel<float><<<kEltBlocks, 256, 0, h->stream>>>((const float *)psi, (float *)tmp, h->nr);
-  CUDA_TRY(h, cudaGetLastError());
+    rc = elt<float>(h, adj_nonlin_kernel<float>, (const float *)u, (const float *)v, (float *)tmp, h->nr, kind,
+                    cf[0], cf[1], cf[2], cf[3], cf[4]);
+  if (rc) return rc;
   if ((rc = fwd_real(h, tmp, c1))) return rc;
-  // lambda_hat = F[lambda_{n+1}]
+  // lambda_hat = F[lambda_{n+1}]; c0 <- opL lambda_hat, c1 <- opN lambda_hat
   if ((rc = fwd_real(h, lam, c0))) return rc;
+  const bool dr = has_r(h);
   if (f64)
     adj_modes_kernel<double><<<h->npartials, 256, 0, h->stream>>>(
         (double2 *)c0, (const double2 *)psi_hat_n, (double2 *)c1, (const double *)h->tab_a,
-        (const double *)h->tab_b, (const double *)h->tab_ar, (const double *)h->tab_br, h->M, h->nyq_off,
-        h->partials);
+        (const double *)h->tab_b, dr ? (const double *)h->tab_ar : nullptr, (const double *)h->tab_br, h->M,
+        h->nyq_off, h->partials);
   else
     adj_modes_kernel<float><<<h->npartials, 256, 0, h->stream>>>(
-        (float2 *)c0, (const float2 *)psi_hat_n, (float2 *)c1, (const float *)h->tab_a,
-        (const float *)h->tab_b, (const float *)h->tab_ar, (const float *)h->tab_br, h->M, h->nyq_off,
-        h->partials);
+        (float2 *)c0, (const float2 *)psi_hat_n, (float2 *)c1, (const float *)h->tab_a, (const float *)h->tab_b,
+        dr ? (const float *)h->tab_ar : nullptr, (const float *)h->tab_br, h->M, h->nyq_off, h->partials);
   CUDA_TRY(h, cudaGetLastError());
-  std::vector<double> part(h->npartials);
-  CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->partials, sizeof(double) * h->npartials,
-                              cudaMemcpyDeviceToHost, h->stream));
-  // u = F^-1[opL lambda_hat] -> lam ; w = F^-1[opN lambda_hat] -> tmp
+  // lam = A lambda ; tmp = w = B lambda ; lam += dN/du w ; v <- g = dN/dv w
   if ((rc = bwd_real(h, c0, lam, 0.0))) return rc;
   if ((rc = bwd_real(h, c1, tmp, 0.0))) return rc;
   if (f64)
-    adj_combine_kernel<double><<<kEltBlocks, 256, 0, h->stream>>>(
-        (const double *)lam, (const double *)psi, (const double *)tmp, (double *)lam, h->nr);
+    rc = elt<double>(h, adj_jacobian_kernel<double>, (const double *)u, (const double *)v, (const double *)tmp,
+                     (double *)lam, (double *)v, h->nr, kind, cf[0], cf[1], cf[2], cf[3], cf[4]);
   else
-    adj_combine_kernel<float><<<kEltBlocks, 256, 0, h->stream>>>(
-        (const float *)lam, (const float *)psi, (const float *)tmp, (float *)lam, h->nr);
-  CUDA_TRY(h, cudaGetLastError());
-  CUDA_TRY(h, cudaStreamSynchronize(h->stream));
-  *dr += neumaier(part.data(), part.size()) / (double)h->nr;
+    rc = elt<float>(h, adj_jacobian_kernel<float>, (const float *)u, (const float *)v, (const float *)tmp,
+                    (float *)lam, (float *)v, h->nr, kind, cf[0], cf[1], cf[2], cf[3], cf[4]);
+  if (rc) return rc;
+  if (kind != 0) {  // lam += C g: the adjoint of the mean-field filter is the filter
+    if ((rc = fwd_real(h, v, c0))) return rc;
+    if ((rc = opfc_scale_by_table(h, c0, h->tab_chi, c0))) return rc;
+    if ((rc = bwd_real(h, c0, tmp, 0.0))) return rc;
+    if (f64)
+      rc = elt<double>(h, adj_add_kernel<double>, (double *)lam, (const double *)tmp, h->nr);
+    else
+      rc = elt<float>(h, adj_add_kernel<float>, (float *)lam, (const float *)tmp, h->nr);
+    if (rc) return rc;
+  }
   return OPFC_OK;
 }
 
@@ -2042,8 +2190,8 @@ int opfc_set_r(opfc_handle *h, double r) {
 
 int opfc_forward_checkpointed(opfc_handle *h, int n_steps, int K) {
   if (!h) return OPFC_ERR_ARG;
-  if (h->desc.model != OPFC_MODEL_PLAIN)
-    return fail(h, OPFC_ERR_ARG, "the adjoint is implemented for the plain PFC model");
+  if (h->al_grad)
+    return fail(h, OPFC_ERR_ARG, "no adjoint for the Aluminum model with a moving temperature gradient");
   if (n_steps < 1 || K < 1) return fail(h, OPFC_ERR_ARG, "need n_steps >= 1 and K >= 1");
   if (!h->initialized || !h->have_state) return fail(h, OPFC_ERR_STATE, "need tables and a state");
   CUDA_TRY(h, cudaSetDevice(h->device));
@@ -2079,7 +2227,7 @@ int opfc_adjoint(opfc_handle *h, const void *grad_psi_T, int dtype, int where, v
   CUDA_TRY(h, cudaMemcpyAsync(h->adj_r[0], h->real_buf, h->nr * h->rsz, cudaMemcpyDeviceToDevice, h->stream));
   const int K = h->ckpt_K, n = h->ckpt_steps;
   const int nseg = (n + K - 1) / K;
-  double dr = 0.0;
+  CUDA_TRY(h, cudaMemsetAsync(h->partials, 0, sizeof(double) * h->npartials, h->stream));
   for (int sg = nseg - 1; sg >= 0; --sg) {
     const int len = std::min(K, n - sg * K);
     // recompute the segment's states with the forward step itself
@@ -2090,7 +2238,15 @@ int opfc_adjoint(opfc_handle *h, const void *grad_psi_T, int dtype, int where, v
       if ((rc = opfc_step(h, 1))) return rc;
     }
     for (int i = len - 1; i >= 0; --i)
-      if ((rc = adjoint_step(h, h->seg[i], &dr))) return rc;
+      if ((rc = adjoint_step(h, h->seg[i]))) return rc;
+  }
+  double dr = std::nan("");  // not a parameter of the model
+  if (has_r(h)) {
+    std::vector<double> part(h->npartials);
+    CUDA_TRY(h, cudaMemcpyAsync(part.data(), h->partials, sizeof(double) * h->npartials, cudaMemcpyDeviceToHost,
+                                h->stream));
+    CUDA_TRY(h, cudaStreamSynchronize(h->stream));
+    dr = neumaier(part.data(), part.size()) / (double)h->nr;
   }
   // leave the handle at the end state of the forward run
   if ((rc = copy_state(h, h->psi_hat, h->ckpt[nseg]))) return rc;

@@ -113,3 +113,14 @@ def test_random_seeds_matches_reference_fixture(oracle, golden_dir, key, case):
     got = ob.ic_random_seeds(n, dx, org, rho, amp)
     np.testing.assert_array_equal(got, np.load(os.path.join(golden_dir, "random_seeds.npz"))[key])
     np.testing.assert_array_equal(got, oracle.ic_random_seeds(n, dx, org, rho, amp))
+
+
+def test_step_kernel_regions_name_the_reference_regions():
+    L = _lib.lib()
+    names = [L.opfc_step_kernel_name(k).decode() for k in range(5)]
+    regions = [L.opfc_step_kernel_region(k).decode() for k in range(5)]
+    assert names == ["y_inverse", "x_fused", "y_forward", "z_update", "hermitian_fix"]
+    # every kernel sits in a region of the reference's step (tungsten_model.hpp:313-362)
+    assert all(r.startswith("gradient/mean_field/") or r.startswith("gradient/evolve/") for r in regions)
+    assert "gradient/evolve/forward + multiply + backward" in regions[3]
+    assert L.opfc_step_kernel_region(5) == b"" and L.opfc_step_kernel_region(-1) == b""

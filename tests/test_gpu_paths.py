@@ -164,3 +164,20 @@ def test_autotune_fp32_computed_operators_on_request(tmp_path, monkeypatch):
     m.initialize(0.5)
     ms = m.autotune()
     assert ms["z.computed"] > 0 and ms["z.direct_computed"] > 0 and ms["z.computed_pingpong"] > 0
+
+
+@pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
+@pytest.mark.parametrize("n", [(1024, 32, 32), (32, 1024, 32), (32, 32, 1024)])
+def test_filtered_1024_axes(oracle, path, prec, tol, n):
+    """Every axis at the measured filtered configuration's length (1024) once,
+    with the others short: 1024-point x rows (M = 512), y lines and z lines
+    (the z update's W = 4 tiles, its one- and two-stage rings, the (ky, N1 - ky)
+    tile order over 1024 rows)."""
+    psi0 = oracle.ic_seeds(n, PI4, -0.10, 0.001, 2, 8.0, 0.2, 6)
+    ref = oracle.run_filtered(psi0, PI4, -0.3, 0.5, -0.1, -0.5, 0.3, 0.5, 6)
+    m = ob.FilteredB200(n, PI4, precision=prec)
+    m.initialize(0.5)
+    m.set_psi(psi0)
+    m.step(6)
+    m.sync()
+    assert rel_l2(m.get_psi(), ref) <= tol

@@ -157,3 +157,14 @@ def test_call_order_errors():
         m.step(1)  # before set_psi
     with pytest.raises(ValueError):
         m.set_psi(np.zeros((16, 16, 8)))
+
+
+def test_nvtx_eager_steps_match_oracle(oracle, monkeypatch):
+    """OPFC_NVTX=1: steps run eagerly inside NVTX ranges named after the
+    reference's regions, with the same results as the graph path."""
+    monkeypatch.setenv("OPFC_NVTX", "1")
+    n = (32, 32, 32)
+    psi0 = oracle.ic_noise(n, -0.285, 0.01, 17)
+    ref = oracle.run_plain(psi0, PI4, -0.25, 0.5, 6)
+    _, psi = run_plain(n, ob.FP64, psi0, 6)
+    assert rel_l2(psi, ref) <= 1e-11
