@@ -187,7 +187,8 @@ const char *opfc_step_kernel_region(int k);
  * exchange buffers | 4 direct with 32 values per thread (N = 512, 1024); x: 0
  * pipelined (warp-square kernel
  * where M = R^2 or 2 R^2) | 1 direct | 2 pipelined without it | 3 warp-square
- * with rows loaded straight into registers (PLAIN, FILTERED); z update:
+ * with rows loaded straight into registers (PLAIN, FILTERED) | 4 as 3 with one
+ * resident CTA per SM fewer (a larger register budget); z update:
  * 0 pipelined with streamed tables | 1 pipelined with radial tables (isotropic
  * grids) | 2 direct with streamed tables | 3 pipelined with operators computed
  * from k^2 | 4 direct with computed operators | 5 as 3 with ping-pong exchange
@@ -203,10 +204,10 @@ const char *opfc_step_kernel_region(int k);
  * evaluate them per mode in the compute precision, so FP32 handles consider
  * them only with OPFC_FP32_COMPUTED_OPERATORS=1 in the environment.
  * ms (OPFC_AUTOTUNE_SLOTS doubles, may be NULL) receives the mean
- * milliseconds per launch of y0 .. y4 x0 .. x3 z0 .. z8 (-1 if not applicable).
+ * milliseconds per launch of y0 .. y4 x0 .. x4 z0 .. z8 (-1 if not applicable).
  * Call after opfc_initialize; the passes run in place, so set the field
  * afterwards.  opfc_variants reports the chosen (y, x, z) variants. */
-#define OPFC_AUTOTUNE_SLOTS 18
+#define OPFC_AUTOTUNE_SLOTS 19
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 

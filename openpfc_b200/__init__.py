@@ -231,7 +231,7 @@ class _ModelBase(_Handle):
         device); returns ms per launch by variant.  Set the field afterwards."""
         names = ["y.pipelined", "y.direct", "y.narrow", "y.pingpong", "y.direct_e32", "x.pipelined", "x.direct",
                  "x.no_square",
-                 "x.square_direct",
+                 "x.square_direct", "x.square_direct_regs",
                  "z.tables", "z.radial", "z.direct", "z.computed", "z.direct_computed", "z.computed_pingpong",
                  "z.folded_pingpong", "z.direct_folded", "z.folded"]
         ms = (ctypes.c_double * len(names))()

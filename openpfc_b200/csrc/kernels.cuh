@@ -835,11 +835,11 @@ static int launch_x_sq(const XLaunch &L, cudaStream_t s) {
   return (int)cudaGetLastError();
 }
 
-template <typename Real, int R, int MODEL, int H>
+template <typename Real, int R, int MODEL, int H, int MINB = (H == 1 ? 4 : 2)>
 static int launch_x_sqd(const XLaunch &L, cudaStream_t s) {
   using Cfg = XSqdCfg<Real, R, MODEL, H>;
   if (L.rows % Cfg::ROWS != 0 || Cfg::SMEM > (size_t)kMaxDynSmem) return -1;
-  auto k = x_sqd_kernel<Real, R, MODEL, H>;
+  auto k = x_sqd_kernel<Real, R, MODEL, H, MINB>;
   static int setup[kDevCache];
   const int occ = kernel_setup(k, Cfg::NT, Cfg::SMEM, setup);
   const int ngroups = L.rows / Cfg::ROWS;
@@ -933,8 +933,15 @@ static int launch_x_m(const XLaunch &L, cudaStream_t s) {
     if constexpr (M == 64 || M == 256 || ((M == 128 || M == 512) && sizeof(Real) == 4)) {
       constexpr int H = (M == 64 || M == 256) ? 1 : 2;
       constexpr int R = (M == 64 || M == 128) ? 8 : 16;
-      if (L.model == MK_PLAIN) rc = launch_x_sqd<Real, R, MK_PLAIN, H>(L, s);
-      if (L.model == MK_FILTERED) rc = launch_x_sqd<Real, R, MK_FILTERED, H>(L, s);
+      // sq_direct 2: one CTA fewer per SM, a larger register budget per thread
+      constexpr int MINB_LOW = (H == 1 ? 4 : 2) - 1;
+      if (L.sq_direct == 2) {
+        if (L.model == MK_PLAIN) rc = launch_x_sqd<Real, R, MK_PLAIN, H, MINB_LOW>(L, s);
+        if (L.model == MK_FILTERED) rc = launch_x_sqd<Real, R, MK_FILTERED, H, MINB_LOW>(L, s);
+      } else {
+        if (L.model == MK_PLAIN) rc = launch_x_sqd<Real, R, MK_PLAIN, H>(L, s);
+        if (L.model == MK_FILTERED) rc = launch_x_sqd<Real, R, MK_FILTERED, H>(L, s);
+      }
     }
     if (rc >= 0) return rc;
   }

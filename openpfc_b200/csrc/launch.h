@@ -128,6 +128,7 @@ struct XLaunch {
   int use_tma;         // X_FUSED: persistent bulk-copy-fed kernel when the size allows
   int no_sq;           // X_FUSED: skip the warp-square kernel (x_sq.cuh) for x_tma.cuh
   int sq_direct;       // X_FUSED: warp-square kernel with rows loaded straight into registers
+                       // (1; 2 = the same with one resident CTA per SM fewer)
   int num_sms;
 };
 

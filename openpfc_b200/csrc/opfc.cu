@@ -39,7 +39,7 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 5, kVarX = 4, kVarZ = 9;
+constexpr int kVarY = 5, kVarX = 5, kVarZ = 9;
 // z-update variants by how they obtain opL / opN
 inline bool z_computed(int v) { return v >= 3 && v <= 5; }  // from k^2 in the compute precision
 inline bool z_folded(int v) { return v >= 6 && v <= 8; }    // folded FP64-built tables
@@ -164,7 +164,8 @@ struct opfc_handle {
   //        values per thread (one exchange per transform at N = 512, 1024);
   // var_x: 0 pipelined (warp-square kernel where it applies), 1 direct,
   //        2 pipelined without the warp-square kernel, 3 warp-square kernel
-  //        with rows loaded straight into registers (PLAIN, FILTERED);
+  //        with rows loaded straight into registers (PLAIN, FILTERED), 4 as 3
+  //        with one resident CTA per SM fewer (more registers per thread);
   // var_z: 0 pipelined with streamed tables, 1 pipelined with radial tables,
   //        2 direct with streamed tables, 3 pipelined with computed operators,
   //        4 direct with computed operators, 5 as 3 with ping-pong exchange
@@ -422,7 +423,7 @@ XLaunch x_base(opfc_handle *h) {
   L.flag = h->flag;
   L.use_tma = h->use_tma && h->var_x != 1;
   L.no_sq = h->var_x == 2;
-  L.sq_direct = h->var_x == 3;
+  L.sq_direct = h->var_x == 3 ? 1 : (h->var_x == 4 ? 2 : 0);
   L.num_sms = h->num_sms;
   return L;
 }

@@ -281,8 +281,9 @@ template <typename Real, int R, int MODEL, int H> struct XSqdCfg {
   static constexpr size_t SMEM = TW + TWS + size_t(ROWS) * EXL * sizeof(C);
 };
 
-template <typename Real, int R, int MODEL, int H>
-__global__ void __launch_bounds__(256, H == 1 ? 4 : 2) x_sqd_kernel(const XArgs<Real> a) {
+// MINB resident CTAs per SM set the register budget (65536 / (256 MINB)).
+template <typename Real, int R, int MODEL, int H, int MINB = (H == 1 ? 4 : 2)>
+__global__ void __launch_bounds__(256, MINB) x_sqd_kernel(const XArgs<Real> a) {
   using Cfg = XSqdCfg<Real, R, MODEL, H>;
   using C = typename CxP<Real>::T;
   constexpr int M = Cfg::M;

@@ -35,7 +35,8 @@ def path(request, monkeypatch):
     (OPFC_Y_VARIANT=3, OPFC_X_VARIANT=3, OPFC_Z_VARIANT=6);
     folded_direct: direct-load z update on the folded tables (OPFC_Z_VARIANT=7);
     folded_nopp: pipelined z update on the folded tables without ping-pong
-    buffers (OPFC_Z_VARIANT=8).
+    buffers (OPFC_Z_VARIANT=8) with the register-loaded x pass at one CTA per
+    SM fewer (OPFC_X_VARIANT=4).
     The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
@@ -66,6 +67,7 @@ def path(request, monkeypatch):
         monkeypatch.setenv("OPFC_Z_VARIANT", "7")
     elif request.param == "folded_nopp":
         monkeypatch.setenv("OPFC_Z_VARIANT", "8")
+        monkeypatch.setenv("OPFC_X_VARIANT", "4")
     return request.param
 
 
