@@ -187,15 +187,18 @@ const char *opfc_step_kernel_region(int k);
  * exchange buffers | 4 direct with 32 values per thread (N = 512, 1024); x: 0
  * pipelined (warp-square kernel
  * where M = R^2 or 2 R^2) | 1 direct | 2 pipelined without it | 3 warp-square
- * with rows loaded straight into registers (PLAIN, FILTERED) | 4 as 3 with one
- * resident CTA per SM fewer (a larger register budget); z update:
+ * with rows loaded straight into registers (PLAIN, FILTERED) | 4 as 3, loading
+ * the next row into registers while the current one is transformed; z update:
  * 0 pipelined with streamed tables | 1 pipelined with radial tables (isotropic
  * grids) | 2 direct with streamed tables | 3 pipelined with operators computed
  * from k^2 | 4 direct with computed operators | 5 as 3 with ping-pong exchange
  * buffers (3-5: PLAIN and FILTERED) | 6 pipelined with the folded tables and
  * ping-pong exchange buffers | 7 direct with the folded tables | 8 pipelined
  * with the folded tables (6-8: every model but the moving-gradient Aluminum
- * and caller-supplied operators);
+ * and caller-supplied operators) | 9 as 8 in one persistent kernel with the next
+ * step's inverse y transform, chained per kx slab through L2 (PLAIN, FILTERED,
+ * N1 == N2; the step then launches no separate y-inverse kernel); each z
+ * candidate is timed together with the inverse y transform that follows it;
  * 3 warm-up + 10 timed launches each), keeps the fastest and caches it per
  * device; opfc_initialize applies cached choices.  Every table variant holds
  * operators built in FP64 on the host and rounded once to the compute
@@ -204,10 +207,10 @@ const char *opfc_step_kernel_region(int k);
  * evaluate them per mode in the compute precision, so FP32 handles consider
  * them only with OPFC_FP32_COMPUTED_OPERATORS=1 in the environment.
  * ms (OPFC_AUTOTUNE_SLOTS doubles, may be NULL) receives the mean
- * milliseconds per launch of y0 .. y4 x0 .. x4 z0 .. z8 (-1 if not applicable).
+ * milliseconds per launch of y0 .. y4 x0 .. x4 z0 .. z9 (-1 if not applicable).
  * Call after opfc_initialize; the passes run in place, so set the field
  * afterwards.  opfc_variants reports the chosen (y, x, z) variants. */
-#define OPFC_AUTOTUNE_SLOTS 19
+#define OPFC_AUTOTUNE_SLOTS 20
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 

@@ -231,9 +231,9 @@ class _ModelBase(_Handle):
         device); returns ms per launch by variant.  Set the field afterwards."""
         names = ["y.pipelined", "y.direct", "y.narrow", "y.pingpong", "y.direct_e32", "x.pipelined", "x.direct",
                  "x.no_square",
-                 "x.square_direct", "x.square_direct_regs",
+                 "x.square_direct", "x.square_direct_prefetch",
                  "z.tables", "z.radial", "z.direct", "z.computed", "z.direct_computed", "z.computed_pingpong",
-                 "z.folded_pingpong", "z.direct_folded", "z.folded"]
+                 "z.folded_pingpong", "z.direct_folded", "z.folded", "z.folded_fused_y_inverse"]
         ms = (ctypes.c_double * len(names))()
         _check(self._h, lib().opfc_autotune(self._h, ms))
         return dict(zip(names, list(ms)))

@@ -74,6 +74,13 @@ struct ColLaunch {
   const void *fold_ops;
   const void *fold_chi;
   long long fold_nyq;
+  // COL_UPDATE with the folded tables: also the next step's inverse y transform,
+  // chained per kx slab through L2 in one persistent kernel (zy_fused.cuh;
+  // PLAIN / FILTERED, N1 == N2).  yseg = the y pass's segments, tmap[4] = the
+  // work array with y boxes, zy_ctr = (M/W + 2) zeroed work counters.
+  int fused_yi;
+  ColSeg yseg[2];
+  int *zy_ctr;
   // COL_PLAIN: half-width tiles (64-byte rows) with two CTAs per SM
   int narrow;
   // ping-pong FFT exchange buffers (one CTA barrier per exchange; one ring
@@ -128,7 +135,7 @@ struct XLaunch {
   int use_tma;         // X_FUSED: persistent bulk-copy-fed kernel when the size allows
   int no_sq;           // X_FUSED: skip the warp-square kernel (x_sq.cuh) for x_tma.cuh
   int sq_direct;       // X_FUSED: warp-square kernel with rows loaded straight into registers
-                       // (1; 2 = the same with one resident CTA per SM fewer)
+                       // (1; 2 = the same, loading the next row during the current one)
   int num_sms;
 };
 

@@ -282,7 +282,10 @@ template <typename Real, int R, int MODEL, int H> struct XSqdCfg {
 };
 
 // MINB resident CTAs per SM set the register budget (65536 / (256 MINB)).
-template <typename Real, int R, int MODEL, int H, int MINB = (H == 1 ? 4 : 2)>
+// PF: the next row's values are loaded into registers while the current row is
+// transformed (each row is read and written by the warp that owns it, so the
+// early read of a later row never races its write).
+template <typename Real, int R, int MODEL, int H, int MINB = (H == 1 ? 4 : 2), bool PF = false>
 __global__ void __launch_bounds__(256, MINB) x_sqd_kernel(const XArgs<Real> a) {
   using Cfg = XSqdCfg<Real, R, MODEL, H>;
   using C = typename CxP<Real>::T;
@@ -314,12 +317,36 @@ __global__ void __launch_bounds__(256, MINB) x_sqd_kernel(const XArgs<Real> a) {
   C *out = reinterpret_cast<C *>(a.out);
   const Real sc = (Real)a.scale, mn = (Real)a.mean;
   bool bad = false;
-  for (long long row0 = (long long)blockIdx.x * ROWS; row0 < a.rows; row0 += (long long)gridDim.x * ROWS) {
+  const long long rstep = (long long)gridDim.x * ROWS;
+  C vn[PF ? E : 1];
+  C nyqn = mk<C>(0, 0);
+  if constexpr (PF) {
+    const long long row = (long long)blockIdx.x * ROWS + c;
+    if (row < a.rows) {
+#pragma unroll
+      for (int m = 0; m < E; ++m) vn[m] = in[row * M + j + R * m];
+      nyqn = in[a.nyq_off + row];
+    }
+  }
+  for (long long row0 = (long long)blockIdx.x * ROWS; row0 < a.rows; row0 += rstep) {
     const long long row = row0 + c;  // rows is a multiple of ROWS (launcher)
     C v[E];
+    C nyq;
+    if constexpr (PF) {
 #pragma unroll
-    for (int m = 0; m < E; ++m) v[m] = in[row * M + j + R * m];
-    const C nyq = in[a.nyq_off + row];
+      for (int m = 0; m < E; ++m) v[m] = vn[m];
+      nyq = nyqn;
+      const long long rn = row + rstep;
+      if (rn < a.rows) {
+#pragma unroll
+        for (int m = 0; m < E; ++m) vn[m] = in[rn * M + j + R * m];
+        nyqn = in[a.nyq_off + rn];
+      }
+    } else {
+#pragma unroll
+      for (int m = 0; m < E; ++m) v[m] = in[row * M + j + R * m];
+      nyq = in[a.nyq_off + row];
+    }
     // natural order into the row buffer: ex[k] = X[k], ex[M] = X[M]
 #pragma unroll
     for (int m = 0; m < E; ++m) ex[j + R * m] = v[m];

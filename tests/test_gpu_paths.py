@@ -15,7 +15,7 @@ PI4 = [math.pi / 4] * 3
 
 
 @pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "pingpong", "e32",
-                        "folded", "folded_direct", "folded_nopp"])
+                        "folded", "folded_direct", "folded_nopp", "fused_zy"])
 def path(request, monkeypatch):
     """tma: pipelined kernels streaming the per-mode tables (default);
     tma_radial: the z update reading radial operator tables (OPFC_Z_VARIANT=1,
@@ -35,8 +35,11 @@ def path(request, monkeypatch):
     (OPFC_Y_VARIANT=3, OPFC_X_VARIANT=3, OPFC_Z_VARIANT=6);
     folded_direct: direct-load z update on the folded tables (OPFC_Z_VARIANT=7);
     folded_nopp: pipelined z update on the folded tables without ping-pong
-    buffers (OPFC_Z_VARIANT=8) with the register-loaded x pass at one CTA per
-    SM fewer (OPFC_X_VARIANT=4).
+    buffers (OPFC_Z_VARIANT=8) with the register-loaded x pass prefetching the
+    next row (OPFC_X_VARIANT=4);
+    fused_zy: the z update on the folded tables fused with the next inverse y
+    transform in one persistent kernel (OPFC_Z_VARIANT=9; PLAIN and FILTERED
+    with N1 == N2, others keep the unfused update 8).
     The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
@@ -68,6 +71,8 @@ def path(request, monkeypatch):
     elif request.param == "folded_nopp":
         monkeypatch.setenv("OPFC_Z_VARIANT", "8")
         monkeypatch.setenv("OPFC_X_VARIANT", "4")
+    elif request.param == "fused_zy":
+        monkeypatch.setenv("OPFC_Z_VARIANT", "9")
     return request.param
 
 
@@ -76,7 +81,8 @@ def rel_l2(a, b):
 
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
-@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 256), (256, 16, 512), (512, 32, 16), (1024, 16, 16)])
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 256), (256, 16, 512), (512, 32, 16), (1024, 16, 16),
+                               (16, 512, 512), (32, 128, 128)])
 def test_plain(oracle, path, prec, tol, n):
     psi0 = oracle.ic_noise(n, -0.285, 0.01, 3)
     ref = oracle.run_plain(psi0, PI4, -0.25, 0.5, 10)
@@ -133,6 +139,7 @@ def test_autotune_then_parity(oracle, tmp_path, monkeypatch):
     ms = m.autotune()
     assert ms["y.pipelined"] > 0 and ms["y.narrow"] > 0 and ms["z.tables"] > 0 and ms["z.radial"] > 0
     assert ms["z.folded_pingpong"] > 0 and ms["z.direct_folded"] > 0 and ms["z.folded"] > 0
+    assert ms["z.folded_fused_y_inverse"] > 0
     # FP32 operators computed per mode are candidates only on request
     assert ms["z.computed"] == -1 and ms["z.direct_computed"] == -1 and ms["z.computed_pingpong"] == -1
     assert m.variants()[2] not in (3, 4, 5)
