@@ -174,7 +174,7 @@ class Clocks:
 def operator_source(var_z):
     if var_z in (3, 4, 5):
         return "opL/opN computed per mode in the compute precision (expm1f, fast divide)"
-    if var_z in (6, 7, 8, 9):
+    if var_z in (6, 7, 8):
         return "FP64-built opL/opN tables rounded to FP32 (folded by the evenness of k^2 in ky, kz)"
     if var_z == 1:
         return "FP64-built opL/opN radial tables rounded to FP32"
@@ -184,11 +184,11 @@ def operator_source(var_z):
 def z_table_bytes(var_z, n, t, st):
     """HBM bytes of operator tables one z update reads: t per-mode tables for
     the table variants (0, 2); the folded tables, (M+1)(N/2+1)^2 modes read once
-    per step (tiles walked in (ky, N - ky) pairs), for 6-9; none for the radial
+    per step (tiles walked in (ky, N - ky) pairs), for 6-8; none for the radial
     (L2-resident) and computed variants."""
     if var_z in (0, 2):
         return (n // 2 + 1) * n * n * t * st
-    if var_z in (6, 7, 8, 9):
+    if var_z in (6, 7, 8):
         return (n // 2 + 1) * (n // 2 + 1) * (n // 2 + 1) * t * st
     return 0
 
@@ -380,12 +380,6 @@ def run_b200(args):
     m.set_psi(psi0_32)
     prof = m.profile_step(reps=args.profile_reps)
     ab = alg_bytes_per_kernel(N, 4, z_table_bytes(m.variants()[2], N, 2, 4))
-    if m.variants()[2] == 9:
-        # z update fused with the next inverse y transform (one kernel; the
-        # intermediate stays in L2, so its HBM bytes are the z update's)
-        prof.pop("y_inverse", None)
-        prof["z_update_y_inverse"] = prof.pop("z_update")
-        ab["z_update_y_inverse"] = ab["z_update"]
     passes = {}
     for k, t in prof.items():
         gbs = ab[k] / (t / 1e3) / 1e9
@@ -398,7 +392,7 @@ def run_b200(args):
             # per-launch DRAM bytes from ncu, keyed "<pass>/v<variant>" (the
             # variant of that pass this run uses)
             var = {"y_inverse": m.variants()[0], "y_forward": m.variants()[0], "x_fused": m.variants()[1],
-                   "z_update": m.variants()[2], "z_update_y_inverse": m.variants()[2]}.get(dom, 0)
+                   "z_update": m.variants()[2]}.get(dom, 0)
             traffic = json.load(open(tpath)).get(f"{dom}/v{var}")
         except Exception:
             traffic = None
@@ -462,14 +456,10 @@ def run_filtered(args):
     prof = m.profile_step(reps=max(2, args.profile_reps // 2))
     var_z = m.variants()[2]
     tab = {0: 3 * nc * 4, 2: 3 * nc * 4}.get(var_z, 0)
-    if var_z in (6, 7, 8, 9):
+    if var_z in (6, 7, 8):
         tab = 3 * 4 * (shape[0] // 2 + 1) * (shape[1] // 2 + 1) * (shape[2] // 2 + 1)
     ab = {"y_inverse": 16 * nc, "x_fused": 16 * nc, "y_forward": 16 * nc,
           "z_update": nc * 32 + tab, "hermitian_fix": 4 * 2 * shape[1] * shape[2] * 8}
-    if var_z == 9:
-        prof.pop("y_inverse", None)
-        prof["z_update_y_inverse"] = prof.pop("z_update")
-        ab["z_update_y_inverse"] = ab["z_update"]
     passes = {k: {"ms": t, "gbs": ab[k] / (t / 1e3) / 1e9, "frac": ab[k] / (t / 1e3) / 1e9 / hbm}
               for k, t in prof.items()}
     line = {"metric": "Mcell-steps/s, filtered PFC 1024^3 FP32", "value": cells * args.steps / (ms / 1e3) / 1e6,

@@ -195,10 +195,7 @@ const char *opfc_step_kernel_region(int k);
  * buffers (3-5: PLAIN and FILTERED) | 6 pipelined with the folded tables and
  * ping-pong exchange buffers | 7 direct with the folded tables | 8 pipelined
  * with the folded tables (6-8: every model but the moving-gradient Aluminum
- * and caller-supplied operators) | 9 as 8 in one persistent kernel with the next
- * step's inverse y transform, chained per kx slab through L2 (PLAIN, FILTERED,
- * N1 == N2; the step then launches no separate y-inverse kernel); each z
- * candidate is timed together with the inverse y transform that follows it;
+ * and caller-supplied operators);
  * 3 warm-up + 10 timed launches each), keeps the fastest and caches it per
  * device; opfc_initialize applies cached choices.  Every table variant holds
  * operators built in FP64 on the host and rounded once to the compute
@@ -207,10 +204,10 @@ const char *opfc_step_kernel_region(int k);
  * evaluate them per mode in the compute precision, so FP32 handles consider
  * them only with OPFC_FP32_COMPUTED_OPERATORS=1 in the environment.
  * ms (OPFC_AUTOTUNE_SLOTS doubles, may be NULL) receives the mean
- * milliseconds per launch of y0 .. y4 x0 .. x4 z0 .. z9 (-1 if not applicable).
+ * milliseconds per launch of y0 .. y4 x0 .. x4 z0 .. z8 (-1 if not applicable).
  * Call after opfc_initialize; the passes run in place, so set the field
  * afterwards.  opfc_variants reports the chosen (y, x, z) variants. */
-#define OPFC_AUTOTUNE_SLOTS 20
+#define OPFC_AUTOTUNE_SLOTS 19
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 

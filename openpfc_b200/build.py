@@ -23,8 +23,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libopenpfc_b200.so")
 SOURCES = ["kernels_f32.cu", "kernels_f64.cu", "ensemble_f32.cu", "ensemble_f64.cu", "opfc.cu", "noalloc.cu",
            "ensemble.cu", "io.cu", "wait_check.cu"]
-HEADERS = ["fft_core.cuh", "kernels.cuh", "launch.h", "col_tma.cuh", "zy_fused.cuh", "x_tma.cuh", "x_sq.cuh",
-           "twiddle.h",
+HEADERS = ["fft_core.cuh", "kernels.cuh", "launch.h", "col_tma.cuh", "x_tma.cuh", "x_sq.cuh", "twiddle.h",
            "ensemble.cuh", "autotune.h", "io.h"]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

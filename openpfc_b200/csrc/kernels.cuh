@@ -104,7 +104,6 @@ template <typename C> __device__ __forceinline__ C czero() { return mk<C>(0, 0);
 }  // namespace opfc
 
 #include "col_tma.cuh"
-#include "zy_fused.cuh"
 
 namespace opfc {
 
@@ -742,55 +741,8 @@ static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
   }
 }
 
-// The z update fused with the next inverse y transform (zy_fused.cuh); -1 when
-// this size / model has no such kernel (the caller then reports an error: the
-// step relies on the y transform being done).
-template <typename Real, int N, int MODEL>
-static int launch_zy(const ColLaunch &L, cudaStream_t s) {
-  using C = typename Cx<Real>::T;
-  constexpr int W = tma_col_width(N, (int)sizeof(C), COL_UPDATE);
-  using Cfg = TmaCfg<Real, N, W, COL_UPDATE, MODEL, OPS_FOLDED, 2, false>;
-  if constexpr (Cfg::STAGES < 1 || N % 16 != 0 || (MODEL != MK_PLAIN && MODEL != MK_FILTERED)) {
-    return -1;
-  } else {
-    if (!L.tmap[0] || !L.tmap[1] || !L.tmap[2] || !L.tmap[4] || !L.zy_ctr || !L.fold_ops) return -1;
-    if (MODEL == MK_FILTERED && !L.tmap[3]) return -1;
-    if (L.seg[0].ncols % W != 0 || L.seg[0].col_stride != 1 || L.yseg[0].ncols % W != 0) return -1;
-    constexpr int NT = W * (N / Plan<N>::E);
-    auto k = zy_kernel<Real, N, W, MODEL>;
-    static int setup[kDevCache];
-    const int occ = kernel_setup(k, NT, Cfg::SMEM, setup);
-    ColArgs<Real> a = col_args<Real>(L);
-    a.seg0 = retile(L.seg[0], W, Width<Real>::W);
-    a.seg1 = retile(L.seg[1], W, Width<Real>::W);
-    ZyArgs z;
-    z.ctr = L.zy_ctr;
-    z.ymain = retile(L.yseg[0], W, Width<Real>::W);
-    z.ynyq = retile(L.yseg[1], W, Width<Real>::W);
-    z.S = L.seg[0].ncols / W;
-    z.BQ = a.seg1.ntiles;
-    z.CQ = z.ynyq.ntiles;
-    if (z.S < 1 || z.BQ < 1 || z.CQ < 1) return -1;
-    const long long total = N + (long long)(z.S - 1) * 2 * N + z.BQ + N + z.CQ;
-    long long G = (long long)(L.num_sms > 0 ? L.num_sms : 148) * occ;  // every CTA resident
-    if (G > total) G = total;
-    cudaError_t e = cudaMemsetAsync(L.zy_ctr, 0, sizeof(int) * (size_t)(z.S + 2), s);
-    if (e != cudaSuccess) return (int)e;
-    const CUtensorMap *m = reinterpret_cast<const CUtensorMap *>(L.tmap[0]);
-    auto pick = [&](int i) { return L.tmap[i] ? *reinterpret_cast<const CUtensorMap *>(L.tmap[i]) : *m; };
-    k<<<(unsigned)G, NT, Cfg::SMEM, s>>>(*m, pick(1), pick(2), pick(3), pick(4), a, z, L.flag);
-    return (int)cudaGetLastError();
-  }
-}
-
 template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
 static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
-  if constexpr (MODE == COL_UPDATE) {
-    if (L.fused_yi) {
-      const int rc = launch_zy<Real, N, MODEL>(L, s);
-      return rc >= 0 ? rc : (int)cudaErrorInvalidValue;
-    }
-  }
   if (L.tmap[0]) {
     int rc;
     if constexpr (MODE == COL_UPDATE)

@@ -74,13 +74,6 @@ struct ColLaunch {
   const void *fold_ops;
   const void *fold_chi;
   long long fold_nyq;
-  // COL_UPDATE with the folded tables: also the next step's inverse y transform,
-  // chained per kx slab through L2 in one persistent kernel (zy_fused.cuh;
-  // PLAIN / FILTERED, N1 == N2).  yseg = the y pass's segments, tmap[4] = the
-  // work array with y boxes, zy_ctr = (M/W + 2) zeroed work counters.
-  int fused_yi;
-  ColSeg yseg[2];
-  int *zy_ctr;
   // COL_PLAIN: half-width tiles (64-byte rows) with two CTAs per SM
   int narrow;
   // ping-pong FFT exchange buffers (one CTA barrier per exchange; one ring

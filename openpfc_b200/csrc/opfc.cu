@@ -39,12 +39,11 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 5, kVarX = 5, kVarZ = 10;
+constexpr int kVarY = 5, kVarX = 5, kVarZ = 9;
 // z-update variants by how they obtain opL / opN
 inline bool z_computed(int v) { return v >= 3 && v <= 5; }  // from k^2 in the compute precision
-inline bool z_folded(int v) { return v >= 6 && v <= 9; }    // folded FP64-built tables
+inline bool z_folded(int v) { return v >= 6 && v <= 8; }    // folded FP64-built tables
 inline bool z_direct(int v) { return v == 2 || v == 4 || v == 7; }
-inline bool z_fused(int v) { return v == 9; }  // with the next inverse y transform (zy_fused.cuh)
 // OPFC_FP32_COMPUTED_OPERATORS=1 lets FP32 handles use (and tune) the update
 // variants that compute opL / opN per mode in FP32 (expm1f, fast divide)
 // instead of reading FP64-built tables rounded to FP32.
@@ -172,11 +171,8 @@ struct opfc_handle {
   //        4 direct with computed operators, 5 as 3 with ping-pong exchange
   //        buffers (3-5: PLAIN and FILTERED), 6 pipelined with the folded
   //        tables and ping-pong exchange buffers, 7 direct with the folded
-  //        tables, 8 pipelined with the folded tables, 9 as 8 fused with the
-  //        next step's inverse y transform (the step then launches no y-inverse
-  //        kernel; PLAIN / FILTERED with N1 == N2)
+  //        tables, 8 pipelined with the folded tables
   int var_y = 0, var_x = 0, var_z = 0;
-  int *zy_ctr = nullptr;  // work counters of the fused z-update / y-inverse kernel
   int num_sms = 148;
   struct Tmap {
     const void *ptr;
@@ -445,8 +441,6 @@ std::string tune_key(const opfc_handle *h, const char *pass) {
   return b;
 }
 
-bool zy_active(const opfc_handle *h);
-
 // A <- F_z^-1[psi_hat] (and, for TUNGSTEN, B <- F_z^-1[chi psi_hat]); FILTERED
 // keeps only the filtered density in A.
 int prepare_a(opfc_handle *h) {
@@ -478,20 +472,8 @@ int prepare_a(opfc_handle *h) {
       LAUNCH_TRY(h, col_plain(h, 2, +1, h->work_c, h->work_c));
     }
   }
-  // with the fused z update, every step ends with A already transformed along
-  // y, so the first step starts from that state too
-  if (zy_active(h)) LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_a, h->work_a));
   h->a_valid = true;
   return OPFC_OK;
-}
-
-// The z update runs fused with the next inverse y transform (z variant 9) and
-// this handle's model and grid allow it.
-bool zy_active(const opfc_handle *h) {
-  const int model = h->desc.model;
-  return z_fused(h->var_z) && (model == OPFC_MODEL_PLAIN || model == OPFC_MODEL_FILTERED) && h->fold_ops &&
-         h->zy_ctr && h->use_tma && h->n1 == h->n2 && h->n2 % 16 == 0 && h->n1 > 1 &&
-         h->M % tma_col_width(h->n2, 2 * (int)h->rsz, COL_UPDATE) == 0;
 }
 
 // Number of kernels one step launches (YI, X, YF, ZU, HERM).
@@ -532,7 +514,7 @@ int enqueue_step(opfc_handle *h, int only = -1) {
 
 int enqueue_step_kernels(opfc_handle *h, int only) {
   const int model = h->desc.model;
-  if ((only < 0 || only == 0) && !zy_active(h)) {  // YI (done by the fused z update otherwise)
+  if (only < 0 || only == 0) {  // YI
     if (two_field(model)) {
       LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_a, h->work_a, h->work_b, h->work_b));
       if (h->al_grad) LAUNCH_TRY(h, col_plain(h, 1, +1, h->work_c, h->work_c));
@@ -627,14 +609,6 @@ int enqueue_step_kernels(opfc_handle *h, int only) {
       Z.fold_chi = h->fold_chi;
       Z.fold_nyq = h->fold_nyq;
     }
-    if (zy_active(h)) {
-      Z.fused_yi = 1;
-      Z.zy_ctr = h->zy_ctr;
-      ColLaunch Y{};
-      col_segments(h, 1, Y);
-      Z.yseg[0] = Y.seg[0];
-      Z.yseg[1] = Y.seg[1];
-    }
     Z.rad_M = h->M;
     Z.rad_n1 = h->n1;
     Z.rad_n2 = h->n2;
@@ -652,9 +626,7 @@ int enqueue_step_kernels(opfc_handle *h, int only) {
       } else if (Z.fold_ops) {
         Z.tmap[2] = tmap_fold(h, h->fold_ops, W, true);
         Z.tmap[3] = h->fold_chi ? tmap_fold(h, h->fold_chi, W, false) : nullptr;
-        if (Z.fused_yi) Z.tmap[4] = tmap_for(h, h->work_a, 1, W, false);
-        if (!Z.tmap[1] || !Z.tmap[2] || (h->fold_chi && !Z.tmap[3]) || (Z.fused_yi && !Z.tmap[4]))
-          Z.tmap[0] = nullptr;
+        if (!Z.tmap[1] || !Z.tmap[2] || (h->fold_chi && !Z.tmap[3])) Z.tmap[0] = nullptr;
       } else if (h->rad_ops && h->var_z == 1) {
         // isotropic grid: operators from the L2-resident radial tables
         Z.rad_ops = h->rad_ops;
@@ -670,7 +642,6 @@ int enqueue_step_kernels(opfc_handle *h, int only) {
         if (!Z.tmap[1] || !Z.tmap[2] || !Z.tmap[3] || (h->tab_chi && !Z.tmap[4])) Z.tmap[0] = nullptr;
       }
     }
-    if (Z.fused_yi && !Z.tmap[0]) return fail(h, OPFC_ERR_CUDA, "fused z update: tensor maps unavailable");
     LAUNCH_TRY(h, col(h, Z));
   }
   if (only < 0 || only == 4) {  // Hermitian projection of the kx = 0 / Nyquist planes
@@ -1056,7 +1027,7 @@ int opfc_destroy(opfc_handle *h) {
     if (p) cudaFree(p);
   void *adj[] = {h->tab_ar,   h->tab_br,   h->adj_c[0], h->adj_c[1], h->adj_r[0], h->adj_r[1],
                  h->adj_r[2], h->adj_r[3], h->rad_ops,  h->rad_chi,  h->tab_p,    h->work_c,
-                 h->time_dev, h->fold_ops, h->fold_chi, h->zy_ctr};
+                 h->time_dev, h->fold_ops, h->fold_chi};
   for (void *p : adj)
     if (p) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -1122,7 +1093,6 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   if ((rc = upload_twiddles(hp, hp->n2, &hp->tw_z))) return cleanup(rc);
   if ((rc = dev_alloc(hp, (void **)&hp->flag, sizeof(unsigned int)))) return cleanup(rc);
   if ((rc = dev_alloc(hp, (void **)&hp->partials, sizeof(double) * hp->npartials))) return cleanup(rc);
-  if ((rc = dev_alloc(hp, (void **)&hp->zy_ctr, sizeof(int) * (size_t)(hp->M / 4 + 2)))) return cleanup(rc);
   if (cudaMemset(hp->flag, 0, sizeof(unsigned int)) != cudaSuccess) return cleanup(OPFC_ERR_CUDA);
   if (cudaMemset(hp->psi_hat, 0, cb) != cudaSuccess) return cleanup(OPFC_ERR_CUDA);
   if (cudaDeviceGetAttribute(&hp->num_sms, cudaDevAttrMultiProcessorCount, hp->device) != cudaSuccess)
@@ -1370,7 +1340,6 @@ static int finish_initialize(opfc_handle *h) {
   if (h->var_z == 1 && !h->rad_ops) h->var_z = 0;
   if (z_computed(h->var_z) && (two_field(model) || user_ops_model(model))) h->var_z = h->var_z == 4 ? 2 : 0;
   if (z_folded(h->var_z) && !h->fold_ops) h->var_z = h->var_z == 7 ? 2 : 0;
-  if (z_fused(h->var_z) && !zy_active(h)) h->var_z = 8;
   if (h->var_y < 0 || h->var_y >= kVarY) h->var_y = 0;
   h->initialized = true;
   h->a_valid = false;
@@ -1603,9 +1572,7 @@ size_t opfc_size_outbox(const opfc_handle *h) { return h ? h->nc : 0; }
 size_t opfc_allocated_bytes(const opfc_handle *h) { return h ? h->allocated : 0; }
 void *opfc_get_stream(const opfc_handle *h) { return h ? (void *)h->stream : nullptr; }
 // (the Aluminum gradient model's y pass launches once more, for P*psi)
-int opfc_kernels_per_step(const opfc_handle *h) {
-  return h ? kStepKernels + (h->al_grad ? 1 : 0) - (zy_active(h) ? 1 : 0) : 0;
-}
+int opfc_kernels_per_step(const opfc_handle *h) { return h ? kStepKernels + (h->al_grad ? 1 : 0) : 0; }
 
 int opfc_autotune(opfc_handle *h, double *ms) {
   if (!h) return OPFC_ERR_ARG;
@@ -1615,12 +1582,8 @@ int opfc_autotune(opfc_handle *h, double *ms) {
   AutoTuner &T = AutoTuner::instance();
   std::vector<double> my, mx, mz;
   // each candidate runs its pass alone, in place on whatever the arrays hold
-  // (the y inverse is timed as its own kernel: the fused z update is off)
-  h->var_z = 0;
   h->var_y = T.tune(tune_key(h, "y"), kVarY, [&](int v) { h->var_y = v; return enqueue_step(h, 0); }, h->stream, &my);
   h->var_x = T.tune(tune_key(h, "x"), kVarX, [&](int v) { h->var_x = v; return enqueue_step(h, 1); }, h->stream, &mx);
-  // every z candidate is timed with the y inverse that follows it (its own
-  // kernel, or inside the fused variant 9), so the times compare like for like
   h->var_z = T.tune(
       tune_key(h, "z"), kVarZ,
       [&](int v) {
@@ -1631,10 +1594,7 @@ int opfc_autotune(opfc_handle *h, double *ms) {
         if (z_computed(v) && h->prec == OPFC_FP32 && !computed_ops_allowed()) return (int)OPFC_ERR_ARG;
         if (z_folded(v) && !h->fold_ops) return (int)OPFC_ERR_ARG;
         h->var_z = v;
-        if (z_fused(v) && !zy_active(h)) return (int)OPFC_ERR_ARG;
-        int rc = enqueue_step(h, 3);
-        if (!rc && !z_fused(v)) rc = enqueue_step(h, 0);
-        return rc;
+        return enqueue_step(h, 3);
       },
       h->stream, &mz);
   CUDA_TRY(h, cudaStreamSynchronize(h->stream));

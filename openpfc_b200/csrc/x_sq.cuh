@@ -49,6 +49,42 @@ template <typename C> __device__ __forceinline__ C shfl_c(C v, int lane) {
   return r;
 }
 
+// Pointwise nonlinearity of the pair of real values packed in one complex
+// (z = x[2p] + i x[2p+1]), with the C2R scale and the mean added first:
+// u = v sc + mn, N = u^3 (PLAIN) or u^2 (c0 + c1 u + c2 u^2) (FILTERED).  `guard`
+// accumulates N * 0, which becomes NaN once any N is infinite or NaN: the pass's
+// non-finite check at one fused multiply-add per value.  The FP32 form (pf2)
+// issues every operation as a packed FP32x2 instruction; the cube rounds as
+// (u u) u either way.
+template <int MODEL, typename C, typename Real>
+__device__ __forceinline__ C x_nonlin(C v, Real sc, Real mn, Real c0, Real c1, Real c2, C &guard) {
+  const Real x = v.x * sc + mn, y = v.y * sc + mn;
+  Real nx, ny;
+  if constexpr (MODEL == MK_FILTERED) {
+    nx = x * x * (c0 + c1 * x + c2 * x * x);
+    ny = y * y * (c0 + c1 * y + c2 * y * y);
+  } else {
+    nx = x * x * x;
+    ny = y * y * y;
+  }
+  guard.x = __fma_rn(nx, Real(0), guard.x);
+  guard.y = __fma_rn(ny, Real(0), guard.y);
+  return mk<C>(nx, ny);
+}
+template <int MODEL>
+__device__ __forceinline__ pf2 x_nonlin(pf2 v, float sc, float mn, float c0, float c1, float c2, pf2 &guard) {
+  const float2 u = __ffma2_rn(f2(v), make_float2(sc, sc), make_float2(mn, mn));
+  const float2 u2 = __fmul2_rn(u, u);
+  float2 n;
+  if constexpr (MODEL == MK_FILTERED) {  // c0 + c1 u + c2 u^2 as (c2 u + c1) u + c0
+    const float2 q = __ffma2_rn(u, make_float2(c2, c2), make_float2(c1, c1));
+    n = __fmul2_rn(u2, __ffma2_rn(q, u, make_float2(c0, c0)));
+  } else {
+    n = __fmul2_rn(u2, u);
+  }
+  guard = p2(__ffma2_rn(n, make_float2(0.f, 0.f), f2(guard)));
+  return p2(n);
+}
 // Length R*R transform of one line held as v[m] = x[j + R m]; same layout on exit.
 template <typename C, int R, int DIR>
 __device__ __forceinline__ void fft_sq(C (&v)[R], C *ex, int j, const C *tws) {
@@ -212,20 +248,10 @@ __global__ void __launch_bounds__(XSqCfg<Real, R, MODEL, H>::W *R) x_sq_kernel(c
     } else {
       __syncthreads();
       fft_sq_dif<C, R, H, +1>(v, ex0, j, tws, tw);
+      C guard = mk<C>(0, 0);
 #pragma unroll
-      for (int m = 0; m < E; ++m) {
-        const Real x = v[m].x * sc + mn, y = v[m].y * sc + mn;
-        Real nx, ny;
-        if constexpr (MODEL == MK_FILTERED) {
-          nx = x * x * (a.c0 + a.c1 * x + a.c2 * x * x);
-          ny = y * y * (a.c0 + a.c1 * y + a.c2 * y * y);
-        } else {
-          nx = x * x * x;
-          ny = y * y * y;
-        }
-        bad |= !(isfinite(nx) && isfinite(ny));
-        v[m] = mk<C>(nx, ny);
-      }
+      for (int m = 0; m < E; ++m) v[m] = x_nonlin<MODEL>(v[m], sc, mn, a.c0, a.c1, a.c2, guard);
+      bad |= isnan(guard.x) || isnan(guard.y);
     }
     fft_sq_dit<C, R, H, -1>(v, ex0, j, tws, tw);
     // R2C post-processing: X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W_N0^k (Z[k] - conj Z[M-k]);
@@ -316,7 +342,7 @@ __global__ void __launch_bounds__(256, MINB) x_sqd_kernel(const XArgs<Real> a) {
   const C *in = reinterpret_cast<const C *>(a.in0);
   C *out = reinterpret_cast<C *>(a.out);
   const Real sc = (Real)a.scale, mn = (Real)a.mean;
-  bool bad = false;
+  C guard = mk<C>(0, 0);  // N * 0 summed over the rows: NaN once any N is not finite
   const long long rstep = (long long)gridDim.x * ROWS;
   C vn[PF ? E : 1];
   C nyqn = mk<C>(0, 0);
@@ -370,19 +396,7 @@ __global__ void __launch_bounds__(256, MINB) x_sqd_kernel(const XArgs<Real> a) {
     __syncwarp();  // row buffer free: it becomes the FFT exchange space
     fft_sq_dif<C, R, H, +1>(v, ex, j, tws, tw);
 #pragma unroll
-    for (int m = 0; m < E; ++m) {
-      const Real x = v[m].x * sc + mn, y = v[m].y * sc + mn;
-      Real nx, ny;
-      if constexpr (MODEL == MK_FILTERED) {
-        nx = x * x * (a.c0 + a.c1 * x + a.c2 * x * x);
-        ny = y * y * (a.c0 + a.c1 * y + a.c2 * y * y);
-      } else {
-        nx = x * x * x;
-        ny = y * y * y;
-      }
-      bad |= !(isfinite(nx) && isfinite(ny));
-      v[m] = mk<C>(nx, ny);
-    }
+    for (int m = 0; m < E; ++m) v[m] = x_nonlin<MODEL>(v[m], sc, mn, a.c0, a.c1, a.c2, guard);
     fft_sq_dit<C, R, H, -1>(v, ex, j, tws, tw);
 #pragma unroll
     for (int m = 0; m < E; ++m) {
@@ -398,7 +412,7 @@ __global__ void __launch_bounds__(256, MINB) x_sqd_kernel(const XArgs<Real> a) {
     if (j == 0) out[a.nyq_off + row] = mk<C>(v[0].x - v[0].y, Real(0));
     __syncwarp();  // exchange space reused by the next row
   }
-  if (bad && a.flag) atomicOr(a.flag, 1u);
+  if ((isnan(guard.x) || isnan(guard.y)) && a.flag) atomicOr(a.flag, 1u);
 }
 
 }  // namespace opfc

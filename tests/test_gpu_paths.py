@@ -15,7 +15,7 @@ PI4 = [math.pi / 4] * 3
 
 
 @pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "pingpong", "e32",
-                        "folded", "folded_direct", "folded_nopp", "fused_zy"])
+                        "folded", "folded_direct", "folded_nopp"])
 def path(request, monkeypatch):
     """tma: pipelined kernels streaming the per-mode tables (default);
     tma_radial: the z update reading radial operator tables (OPFC_Z_VARIANT=1,
@@ -36,10 +36,7 @@ def path(request, monkeypatch):
     folded_direct: direct-load z update on the folded tables (OPFC_Z_VARIANT=7);
     folded_nopp: pipelined z update on the folded tables without ping-pong
     buffers (OPFC_Z_VARIANT=8) with the register-loaded x pass prefetching the
-    next row (OPFC_X_VARIANT=4);
-    fused_zy: the z update on the folded tables fused with the next inverse y
-    transform in one persistent kernel (OPFC_Z_VARIANT=9; PLAIN and FILTERED
-    with N1 == N2, others keep the unfused update 8).
+    next row (OPFC_X_VARIANT=4).
     The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
@@ -71,8 +68,6 @@ def path(request, monkeypatch):
     elif request.param == "folded_nopp":
         monkeypatch.setenv("OPFC_Z_VARIANT", "8")
         monkeypatch.setenv("OPFC_X_VARIANT", "4")
-    elif request.param == "fused_zy":
-        monkeypatch.setenv("OPFC_Z_VARIANT", "9")
     return request.param
 
 
@@ -139,7 +134,6 @@ def test_autotune_then_parity(oracle, tmp_path, monkeypatch):
     ms = m.autotune()
     assert ms["y.pipelined"] > 0 and ms["y.narrow"] > 0 and ms["z.tables"] > 0 and ms["z.radial"] > 0
     assert ms["z.folded_pingpong"] > 0 and ms["z.direct_folded"] > 0 and ms["z.folded"] > 0
-    assert ms["z.folded_fused_y_inverse"] > 0
     # FP32 operators computed per mode are candidates only on request
     assert ms["z.computed"] == -1 and ms["z.direct_computed"] == -1 and ms["z.computed_pingpong"] == -1
     assert m.variants()[2] not in (3, 4, 5)
