@@ -90,6 +90,13 @@ typedef struct opfc_desc {
   void *stream;        /* cudaStream_t to use, or NULL for a private stream */
   int device;          /* CUDA device ordinal */
   opfc_aluminum_params aluminum; /* ALUMINUM */
+  /* Slab of a grid shared by several handles (sharded step, opfc_pass):
+   * n_global = the whole grid (0 = the handle's own n), kx0 = first global kx
+   * of the handle's half-spectrum columns.  The handle's operators use the
+   * global wave numbers (kx0 + kx) 2 pi / (dx n_global) and its C2R scales by
+   * 1 / (N0 N1 N2 of n_global).  PLAIN and FILTERED. */
+  int n_global[3];
+  int kx0;
 } opfc_desc;
 
 typedef struct opfc_handle opfc_handle;
@@ -130,6 +137,47 @@ int opfc_step(opfc_handle *h, int n_steps);
 /* Wait for the handle's stream; reports OPFC_ERR_NONFINITE if any step
  * produced NaN/Inf since the last check. */
 int opfc_sync(opfc_handle *h);
+
+/* One pass of the step, or of a transform, on the handle's own arrays, queued
+ * on its stream (no counterpart in the reference, whose GPU model runs whole
+ * 3D transforms; these are the pieces a sharded step is built from -- a field
+ * split over ranks in z slabs for the x and y passes and in kx slabs for the z
+ * update, with all-to-all transposes between them, the decomposition of the
+ * reference's HeFFTe plans, src/openpfc/runtime/cpu/fft.cpp:72-81).  PLAIN,
+ * FILTERED and USER_ETD.  Arrays (opfc_array): WORK = A, the half spectrum in
+ * the split layout (main part (N0/2) x N1 x N2 complex, kx fastest, then the
+ * kx = N0/2 plane N1 x N2); STATE = psi_hat, same layout; REAL = N0 N1 N2 reals,
+ * x fastest.  Passes (`mean`: the mean density the x passes add; `flags`):
+ *   Y_INVERSE, Y_FORWARD       A along y, in place
+ *   X_FUSED                    A: per x row C2R, nonlinearity (+ mean), R2C
+ *   Z_UPDATE                   A -> psi_hat (ETD update) and A = F_z^-1 of the
+ *                              new state; then the Hermitian projection of the
+ *                              kx = 0 plane (flags bit 0) and of the kx = N0/2
+ *                              plane (bit 1) -- give only the planes the handle
+ *                              holds of the whole grid
+ *   XY_FORWARD                 REAL -> A: x R2C, y forward
+ *   XY_BACKWARD                A -> REAL: y inverse, x C2R scaled by 1/(N0 N1 N2
+ *                              of n_global), + mean
+ *   Z_FORWARD                  A -> psi_hat (flags bit 2: zero the k = 0 slot)
+ *   Z_INVERSE                  psi_hat -> A as a step starts from it (chi psi_hat
+ *                              for FILTERED)
+ *   Z_INVERSE_STATE            psi_hat -> A
+ * opfc_array returns a device pointer (REAL is allocated on first use), NULL
+ * for a bad argument. */
+#define OPFC_PASS_Y_INVERSE 0
+#define OPFC_PASS_X_FUSED 1
+#define OPFC_PASS_Y_FORWARD 2
+#define OPFC_PASS_Z_UPDATE 3
+#define OPFC_PASS_XY_FORWARD 4
+#define OPFC_PASS_XY_BACKWARD 5
+#define OPFC_PASS_Z_FORWARD 6
+#define OPFC_PASS_Z_INVERSE 7
+#define OPFC_PASS_Z_INVERSE_STATE 8
+#define OPFC_ARRAY_WORK 0
+#define OPFC_ARRAY_STATE 1
+#define OPFC_ARRAY_REAL 2
+int opfc_pass(opfc_handle *h, int pass, double mean, int flags);
+void *opfc_array(opfc_handle *h, int which);
 
 /* Failure-path check (no reference counterpart; the reference's GPU model
  * blocks in cudaDeviceSynchronize without a limit): runs the bounded mbarrier

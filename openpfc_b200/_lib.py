@@ -57,7 +57,8 @@ class Desc(ctypes.Structure):
                 ("filter_alpha", ctypes.c_double), ("p2", ctypes.c_double),
                 ("p3", ctypes.c_double), ("p4", ctypes.c_double),
                 ("tungsten", TungstenParams), ("stream", ctypes.c_void_p),
-                ("device", ctypes.c_int), ("aluminum", AluminumParams)]
+                ("device", ctypes.c_int), ("aluminum", AluminumParams),
+                ("n_global", ctypes.c_int * 3), ("kx0", ctypes.c_int)]
 
 
 class OpfcError(RuntimeError):
@@ -150,6 +151,9 @@ def lib():
     L.opfc_ensemble_stream.restype = vp
     L.opfc_autotune.argtypes = [H, dp]
     L.opfc_check_bounded_wait.argtypes = [H, cd]
+    L.opfc_pass.argtypes = [H, ci, cd, ci]
+    L.opfc_array.argtypes = [H, ci]
+    L.opfc_array.restype = vp
     L.opfc_variants.argtypes = [H, ip]
     L.opfc_set_r.argtypes = [H, cd]
     L.opfc_forward_checkpointed.argtypes = [H, ci, ci]

@@ -1011,11 +1011,20 @@ template <typename Real> int launch_x(const XLaunch &L, cudaStream_t s) {
 
 template <typename Real>
 int launch_herm_fix(void *psi, long long nyq_off, int M, int n1, int n2, cudaStream_t s, double *time,
-                    double dt_time) {
+                    double dt_time, int planes) {
   const long long plane = (long long)n1 * n2;
-  dim3 grid((unsigned)((plane + 255) / 256), 2);
-  herm_fix_kernel<Real><<<grid, 256, 0, s>>>(reinterpret_cast<typename Cx<Real>::T *>(psi), nyq_off,
-                                             M, n1, n2, time, dt_time);
+  using C = typename Cx<Real>::T;
+  C *p = reinterpret_cast<C *>(psi);
+  if ((planes & 3) == 3) {
+    dim3 grid((unsigned)((plane + 255) / 256), 2);
+    herm_fix_kernel<Real><<<grid, 256, 0, s>>>(p, nyq_off, M, n1, n2, time, dt_time);
+  } else if (planes & 1) {  // the kx = 0 plane only (stride M)
+    herm_fix_kernel<Real><<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(p, nyq_off, M, n1, n2, time, dt_time);
+  } else if (planes & 2) {  // the Nyquist plane only: its rows are contiguous (stride 1)
+    herm_fix_kernel<Real><<<(unsigned)((plane + 255) / 256), 256, 0, s>>>(p + nyq_off, 0, 1, n1, n2, time, dt_time);
+  } else if (time) {  // no plane: only the device time advances
+    herm_fix_kernel<Real><<<1, 1, 0, s>>>(p, nyq_off, M, 0, 0, time, dt_time);
+  }
   return (int)cudaGetLastError();
 }
 
@@ -1092,7 +1101,7 @@ int launch_energy_k(const void *psi_hat, int M, int n1, int n2, long long nyq_of
 #define OPFC_INSTANTIATE(R)                                                                          \
   template int launch_col<R>(const ColLaunch &, cudaStream_t);                                       \
   template int launch_x<R>(const XLaunch &, cudaStream_t);                                           \
-  template int launch_herm_fix<R>(void *, long long, int, int, int, cudaStream_t, double *, double);  \
+  template int launch_herm_fix<R>(void *, long long, int, int, int, cudaStream_t, double *, double, int);  \
   template int launch_to_ref<R>(const void *, void *, int, int, int, int, long long, int, double,    \
                                 cudaStream_t);                                                       \
   template int launch_from_ref<R>(const void *, int, void *, int, int, int, long long, cudaStream_t); \
@@ -1107,7 +1116,7 @@ int launch_energy_k(const void *psi_hat, int M, int n1, int n2, long long nyq_of
 #define OPFC_EXTERN(R)                                                                                      \
   extern template int launch_col<R>(const ColLaunch &, cudaStream_t);                                       \
   extern template int launch_x<R>(const XLaunch &, cudaStream_t);                                           \
-  extern template int launch_herm_fix<R>(void *, long long, int, int, int, cudaStream_t, double *, double);  \
+  extern template int launch_herm_fix<R>(void *, long long, int, int, int, cudaStream_t, double *, double, int);  \
   extern template int launch_to_ref<R>(const void *, void *, int, int, int, int, long long, int, double,    \
                                        cudaStream_t);                                                       \
   extern template int launch_from_ref<R>(const void *, int, void *, int, int, int, long long, cudaStream_t); \

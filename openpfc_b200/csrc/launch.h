@@ -163,9 +163,10 @@ int launch_wait_check(unsigned *flag, double limit_ms, cudaStream_t s);
 // Kernel launchers (kernels_f32.cu / kernels_f64.cu).  Return cudaError_t as int.
 template <typename Real> int launch_col(const ColLaunch &a, cudaStream_t s);
 template <typename Real> int launch_x(const XLaunch &a, cudaStream_t s);
+// planes: bit 0 the kx = 0 plane, bit 1 the Nyquist plane
 template <typename Real>
 int launch_herm_fix(void *psi, long long nyq_off, int M, int n1, int n2, cudaStream_t s,
-                    double *time = nullptr, double dt_time = 0.0);
+                    double *time = nullptr, double dt_time = 0.0, int planes = 3);
 template <typename Real>
 int launch_to_ref(const void *in, void *out, int out_is_f64, int M, int n1, int n2,
                   long long nyq_off, int dc_override, double dc_re, cudaStream_t s);

@@ -103,6 +103,13 @@ struct DevBuf {
 struct opfc_handle {
   opfc_desc desc{};
   int n0 = 0, n1 = 0, n2 = 0, M = 0;
+  // the whole grid this handle is a slab of (its own n otherwise) and the
+  // global index of its first half-spectrum column
+  int g0 = 0, g1 = 0, g2 = 0, kx0 = 0;
+  bool slab = false;
+  // opfc_pass: the mean density the x pass adds (the whole grid's, for a slab)
+  bool use_pass_mean = false;
+  double pass_mean = 0.0;
   size_t nr = 0, nc = 0;
   long long nyq_off = 0;
   int prec = OPFC_FP32;
@@ -418,7 +425,7 @@ XLaunch x_base(opfc_handle *h) {
   L.rows = h->n1 * h->n2;
   L.nyq_off = h->nyq_off;
   L.tw = h->tw_x;
-  L.scale = 1.0 / ((double)h->n0 * h->n1 * h->n2);
+  L.scale = 1.0 / ((double)h->g0 * h->g1 * h->g2);
   L.mean = 0.0;
   L.flag = h->flag;
   L.use_tma = h->use_tma && h->var_x != 1;
@@ -527,7 +534,7 @@ int enqueue_step_kernels(opfc_handle *h, int only) {
     X.mode = X_FUSED;
     X.in0 = h->work_a;
     X.out = h->work_a;
-    X.mean = mean_density(h);
+    X.mean = h->use_pass_mean ? h->pass_mean : mean_density(h);
     if (model == OPFC_MODEL_PLAIN) {
       X.model = MK_PLAIN;
     } else if (model == OPFC_MODEL_FILTERED || user_ops_model(model)) {
@@ -1052,6 +1059,16 @@ int opfc_create(const opfc_desc *d, opfc_handle **out) {
   h->n1 = d->n[1];
   h->n2 = d->n[2];
   h->M = h->n0 / 2;
+  h->g0 = d->n_global[0] > 0 ? d->n_global[0] : h->n0;
+  h->g1 = d->n_global[1] > 0 ? d->n_global[1] : h->n1;
+  h->g2 = d->n_global[2] > 0 ? d->n_global[2] : h->n2;
+  h->kx0 = d->kx0;
+  h->slab = h->g0 != h->n0 || h->g1 != h->n1 || h->g2 != h->n2 || h->kx0 != 0;
+  if (h->slab) {
+    if (d->model != OPFC_MODEL_PLAIN && d->model != OPFC_MODEL_FILTERED) return OPFC_ERR_ARG;
+    if (h->g0 % 2 != 0 || h->kx0 < 0 || h->kx0 + h->M > h->g0 / 2 || h->n1 > h->g1 || h->n2 > h->g2)
+      return OPFC_ERR_SIZE;
+  }
   h->nr = (size_t)h->n0 * h->n1 * h->n2;
   h->nc = (size_t)(h->M + 1) * h->n1 * h->n2;
   h->nyq_off = (long long)h->M * h->n1 * h->n2;
@@ -1113,7 +1130,10 @@ int opfc_initialize(opfc_handle *h, double dt) {
     h->dt = dt;
     return finish_initialize(h);
   }
-  const int n0 = h->n0, n1 = h->n1, n2 = h->n2, H = h->M + 1;
+  // a slab handle (opfc_pass) takes its wave numbers from the whole grid: the
+  // half-spectrum column kx is the global column kx0 + kx; its y and z axes
+  // span the whole grid whenever it runs a z update
+  const int n0 = h->g0, n1 = h->n1, n2 = h->n2, H = h->M + 1, kxo = h->kx0;
   const double f0 = 2.0 * kPi / (h->desc.dx[0] * n0);
   const double f1 = 2.0 * kPi / (h->desc.dx[1] * n1);
   const double f2 = 2.0 * kPi / (h->desc.dx[2] * n2);
@@ -1195,7 +1215,7 @@ int opfc_initialize(opfc_handle *h, double dt) {
   parallel_for((long)n2 * n1, [&](long row) {
     const int ky = (int)(row % n1), kz = (int)(row / n1);
     for (int kx = 0; kx < H; ++kx) {
-      const double kx_ = kc(kx, n0, f0), ky_ = kc(ky, n1, f1), kz_ = kc(kz, n2, f2);
+      const double kx_ = kc(kx + kxo, n0, f0), ky_ = kc(ky, n1, f1), kz_ = kc(kz, n2, f2);
       const size_t o = split_index(h, kx, ky, kz);
       double oc = 1.0;
       mode_ops(kx_, ky_, kz_, ta[o], tb[o], oc);
@@ -1221,7 +1241,7 @@ int opfc_initialize(opfc_handle *h, double dt) {
       for (int kx = 0; kx < H; ++kx) {
         const size_t o = kx < h->M ? (size_t)kx + (size_t)h->M * row : (size_t)h->fold_nyq + row;
         double oc = 1.0;
-        mode_ops(kc(kx, n0, f0), fy * f1, fz * f2, fo[2 * o], fo[2 * o + 1], oc);
+        mode_ops(kc(kx + kxo, n0, f0), fy * f1, fz * f2, fo[2 * o], fo[2 * o + 1], oc);
         if (need_chi) fc[o] = oc;
       }
     });
@@ -1270,7 +1290,7 @@ int opfc_initialize(opfc_handle *h, double dt) {
   // the fused z update reads small L2-resident tables instead of streaming the
   // per-mode tables from HBM.  Same formulas, FP64, rounded once.
   const char *no_rad = std::getenv("OPFC_NO_RADIAL");
-  if (f0 == f1 && f1 == f2 && !(no_rad && no_rad[0] == '1') && !h->al_grad) {
+  if (f0 == f1 && f1 == f2 && !(no_rad && no_rad[0] == '1') && !h->al_grad && !h->slab) {
     const long mmax = (long)(n0 / 2) * (n0 / 2) + (long)(n1 / 2) * (n1 / 2) + (long)(n2 / 2) * (n2 / 2);
     const size_t cnt = (size_t)mmax + 1;
     std::vector<double> ops(2 * cnt), chi(need_chi ? cnt : 0);
@@ -1338,7 +1358,8 @@ static int finish_initialize(opfc_handle *h) {
   if (h->var_x < 0 || h->var_x >= kVarX) h->var_x = 0;
   if (h->var_z < 0 || h->var_z >= kVarZ) h->var_z = 0;
   if (h->var_z == 1 && !h->rad_ops) h->var_z = 0;
-  if (z_computed(h->var_z) && (two_field(model) || user_ops_model(model))) h->var_z = h->var_z == 4 ? 2 : 0;
+  if (z_computed(h->var_z) && (two_field(model) || user_ops_model(model) || h->slab))
+    h->var_z = h->var_z == 4 ? 2 : 0;
   if (z_folded(h->var_z) && !h->fold_ops) h->var_z = h->var_z == 7 ? 2 : 0;
   if (h->var_y < 0 || h->var_y >= kVarY) h->var_y = 0;
   h->initialized = true;
@@ -1468,6 +1489,74 @@ int opfc_sync(opfc_handle *h) {
   return OPFC_OK;
 }
 
+int opfc_pass(opfc_handle *h, int pass, double mean, int flags) {
+  if (!h) return OPFC_ERR_ARG;
+  if (pass < OPFC_PASS_Y_INVERSE || pass > OPFC_PASS_Z_INVERSE_STATE) return fail(h, OPFC_ERR_ARG, "unknown pass");
+  if (pass == OPFC_PASS_Z_UPDATE && !h->initialized) return fail(h, OPFC_ERR_STATE, "the z update needs opfc_initialize");
+  if (two_field(h->desc.model) || h->al_grad) return fail(h, OPFC_ERR_ARG, "opfc_pass: PLAIN, FILTERED or USER_ETD");
+  CUDA_TRY(h, cudaSetDevice(h->device));
+  int rc = OPFC_OK;
+  release_graph(h);  // the step graph, if any, bakes in the handle's own mean
+  switch (pass) {
+    case OPFC_PASS_Y_INVERSE:
+      return enqueue_step_kernels(h, 0);
+    case OPFC_PASS_X_FUSED:
+      h->use_pass_mean = true;
+      h->pass_mean = mean;
+      rc = enqueue_step_kernels(h, 1);
+      h->use_pass_mean = false;
+      return rc;
+    case OPFC_PASS_Y_FORWARD:
+      return enqueue_step_kernels(h, 2);
+    case OPFC_PASS_Z_UPDATE: {
+      if ((rc = enqueue_step_kernels(h, 3))) return rc;
+      const int planes = flags & 3;
+      if (h->prec == OPFC_FP64)
+        LAUNCH_TRY(h, launch_herm_fix<double>(h->psi_hat, h->nyq_off, h->M, h->n1, h->n2, h->stream, nullptr, 0.0,
+                                              planes));
+      else
+        LAUNCH_TRY(h, launch_herm_fix<float>(h->psi_hat, h->nyq_off, h->M, h->n1, h->n2, h->stream, nullptr, 0.0,
+                                             planes));
+      return OPFC_OK;
+    }
+    case OPFC_PASS_XY_FORWARD: {  // real_buf -> A: x R2C, y forward
+      if ((rc = ensure_real_buf(h))) return rc;
+      XLaunch X = x_base(h);
+      X.mode = X_R2C;
+      X.rin = h->real_buf;
+      X.out = h->work_a;
+      LAUNCH_TRY(h, xpass(h, X));
+      LAUNCH_TRY(h, col_plain(h, 1, -1, h->work_a, h->work_a));
+      return OPFC_OK;
+    }
+    case OPFC_PASS_XY_BACKWARD:  // A -> real_buf: y inverse, x C2R (scaled by the whole grid), + mean
+      return backward_to_real_buf(h, h->work_a, mean, true);
+    case OPFC_PASS_Z_FORWARD:  // A -> psi_hat
+      LAUNCH_TRY(h, col_plain(h, 2, -1, h->work_a, h->psi_hat));
+      if (flags & 4) CUDA_TRY(h, cudaMemsetAsync(h->psi_hat, 0, 2 * h->rsz, h->stream));
+      h->have_state = true;
+      h->a_valid = false;
+      return OPFC_OK;
+    case OPFC_PASS_Z_INVERSE:  // psi_hat -> A as the step starts (chi-filtered for FILTERED)
+      return prepare_a(h);
+    case OPFC_PASS_Z_INVERSE_STATE:  // psi_hat -> A, unfiltered
+      LAUNCH_TRY(h, col_plain(h, 2, +1, h->psi_hat, h->work_a));
+      return OPFC_OK;
+  }
+  return OPFC_ERR_ARG;
+}
+
+void *opfc_array(opfc_handle *h, int which) {
+  if (!h) return nullptr;
+  if (which == OPFC_ARRAY_WORK) return h->work_a;
+  if (which == OPFC_ARRAY_STATE) return h->psi_hat;
+  if (which == OPFC_ARRAY_REAL) {
+    if (cudaSetDevice(h->device) != cudaSuccess || ensure_real_buf(h)) return nullptr;
+    return h->real_buf;
+  }
+  return nullptr;
+}
+
 int opfc_check_bounded_wait(opfc_handle *h, double limit_ms) {
   if (!h) return OPFC_ERR_ARG;
   if (!(limit_ms >= 0.1 && limit_ms <= 1000.0)) return fail(h, OPFC_ERR_ARG, "limit_ms must be in [0.1, 1000]");
@@ -1588,7 +1677,8 @@ int opfc_autotune(opfc_handle *h, double *ms) {
       tune_key(h, "z"), kVarZ,
       [&](int v) {
         if (v == 1 && !h->rad_ops) return (int)OPFC_ERR_ARG;
-        if (z_computed(v) && (two_field(h->desc.model) || user_ops_model(h->desc.model))) return (int)OPFC_ERR_ARG;
+        if (z_computed(v) && (two_field(h->desc.model) || user_ops_model(h->desc.model) || h->slab))
+          return (int)OPFC_ERR_ARG;
         // FP32: operators computed in FP32 only when the caller opts in; the
         // default keeps FP64-built tables rounded once to the compute precision
         if (z_computed(v) && h->prec == OPFC_FP32 && !computed_ops_allowed()) return (int)OPFC_ERR_ARG;
