@@ -633,6 +633,59 @@ def run_adjoint(args):
     return 0
 
 
+def run_axes(args):
+    """Plain batched transforms along y and along z on a --n cube, FP32 (in
+    place along y; z from A into psi_hat): the same TMA-fed column kernel on
+    both axes, so the gap between them is the cost of the axis's stride (kz
+    rows are one kz plane apart: 4 MB at 1024^3).  10 launches per region after
+    --warmup launches, median of --repeats regions; 16 B of traffic per mode."""
+    import torch
+    import openpfc_b200 as ob
+    from openpfc_b200._lib import lib
+    n = N
+    m = ob.PfcB200((n, n, n), DX, r=R, precision=ob.FP32)
+    m.initialize(DT)
+    tune = None if args.no_autotune else m.autotune()
+    psi = torch.full((n, n, n), N0, dtype=torch.float32, device="cuda")
+    psi += AMP * torch.rand_like(psi)
+    m.set_psi(psi)
+    m.sync()
+    del psi
+    stream = torch.cuda.ExternalStream(m.stream)
+    nc = (n // 2 + 1) * n * n
+    hbm, kind = peaks()
+    out = {}
+    for name, p in (("y_forward", 2), ("z_forward", 6)):
+        for _ in range(args.warmup):
+            _check_rc(lib().opfc_pass(m._h, p, 0.0, 0))
+        regions = []
+        for _ in range(args.repeats):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record(stream)
+            for _ in range(10):
+                _check_rc(lib().opfc_pass(m._h, p, 0.0, 0))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            regions.append(e0.elapsed_time(e1) / 10)
+        ms = statistics.median(regions)
+        gbs = 16 * nc / (ms / 1e3) / 1e9
+        out[name] = {"ms": ms, "gbs": gbs, "frac": gbs / hbm}
+    line = {"metric": f"plain y and z transforms, {n}^3 FP32 (GB/s on 16 B per mode)", "unit": "GB/s",
+            "value": out["z_forward"]["gbs"], "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic", "peak": hbm, "peak_kind": kind, "axes": out,
+            "kz_row_stride_bytes": (n // 2) * n * 8, "variants_yxz": m.variants(),
+            "autotune": tune is not None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _check_rc(rc):
+    if rc != 0:
+        raise RuntimeError(f"opfc_pass returned {rc}")
+
+
 def main(argv=None):
     argv = sys.argv[1:] if argv is None else argv
     ap = argparse.ArgumentParser()
@@ -650,10 +703,11 @@ def main(argv=None):
     ap.add_argument("--profile-reps", type=int, default=10)
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the cached (or default) kernel variants instead of timing them first")
-    ap.add_argument("--workload", default="plain", choices=["plain", "filtered", "ensemble", "adjoint"],
+    ap.add_argument("--workload", default="plain", choices=["plain", "filtered", "ensemble", "adjoint", "axes"],
                     help="plain: the measured 512^3 line; filtered: mean-field-filtered 1024^3 FP32; "
                          "ensemble: 256 uneven members, 50 steps in one graph; adjoint: 128^3 FP32 "
-                         "calibration (200 steps, snapshots every 20)")
+                         "calibration (200 steps, snapshots every 20); axes: plain y and z transforms "
+                         "of an --n cube")
     ap.add_argument("--shape", type=int, nargs=3, default=None, metavar=("N0", "N1", "N2"),
                     help="filtered workload only: a non-cubic grid (for profiling one pass on a small case)")
     ap.add_argument("--dry-run", action="store_true",
@@ -678,6 +732,8 @@ def main(argv=None):
         return run_ensemble(args)
     if args.workload == "adjoint":
         return run_adjoint(args)
+    if args.workload == "axes":
+        return run_axes(args)
     return run_b200(args)
 
 
