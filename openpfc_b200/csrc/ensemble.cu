@@ -121,7 +121,10 @@ int launch_stage(opfc_ensemble *e, int stage, int variant) {
   // prefix sums per stage: y columns (YI, YF), z columns (ZU), x rows (X)
   const int which = stage == 1 ? 2 : (stage == 3 ? 1 : 0);
   const int *p = stage == 4 ? nullptr : pre[which];
-  const int tiles = stage == 4 ? 0 : e->total[wi][which];
+  // the Hermitian fix takes the largest instance's n1 * n2 in place of a tile count
+  int tiles = stage == 4 ? 0 : e->total[wi][which];
+  if (stage == 4)
+    for (const auto &in : e->inst) tiles = std::max(tiles, in.n1 * in.n2);
   const EnsArgs a = args(e, p, stage == 4 ? nullptr : e->d_order[which]);
   return e->prec == OPFC_FP64 ? ens_launch_stage<double>(stage, W, G, e->num_sms, tiles, e->count, a, e->stream)
                               : ens_launch_stage<float>(stage, W, G, e->num_sms, tiles, e->count, a, e->stream);

@@ -268,13 +268,17 @@ __global__ void __launch_bounds__(W *kEnsT, G) ens_x_kernel(const EnsArgs a) {
   if (bad && a.flag) atomicOr(a.flag, 1u);
 }
 
-// Hermitian projection of every instance's kx = 0 and Nyquist planes.
+// Hermitian projection of every instance's kx = 0 and Nyquist planes.  One
+// thread per mode of the two planes (blockIdx.y = instance; the grid's x extent
+// covers the largest instance, so each thread makes one pass: the loop below
+// runs more than once only for a grid sized smaller than that).
 template <typename Real>
 __global__ void ens_herm_kernel(const EnsArgs a) {
   using C = typename Cx<Real>::T;
   const int i = blockIdx.y;
   const EnsInst in = a.inst[i];
   const long long plane = (long long)in.n1 * in.n2;
+  if ((long long)blockIdx.x * blockDim.x >= 2 * plane) return;
   C *psi = reinterpret_cast<C *>(a.psi_hat) + in.off_c;
   const long long nyq = (long long)in.M * plane;
   for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < 2 * plane;
@@ -336,7 +340,9 @@ int ens_launch_stage_w(int stage, int num_sms, int tiles, int count, const EnsAr
     static int setup[kDevCache];
     return ens_persistent(ens_x_kernel<Real, W, G>, G, num_sms, tiles, ens_x_smem<Real, W>(), NT, s, setup, a);
   } else {
-    ens_herm_kernel<Real><<<dim3(8, count), 256, 0, s>>>(a);
+    // `tiles` = the largest instance's n1 * n2 (one thread per mode of its two planes)
+    const int bx = tiles > 0 ? (2 * tiles + 255) / 256 : 8;
+    ens_herm_kernel<Real><<<dim3(bx, count), 256, 0, s>>>(a);
   }
   return (int)cudaGetLastError();
 }
