@@ -174,7 +174,7 @@ class Clocks:
 def operator_source(var_z):
     if var_z in (3, 4, 5):
         return "opL/opN computed per mode in the compute precision (expm1f, fast divide)"
-    if var_z in (6, 7, 8):
+    if var_z in (6, 7, 8, 9):
         return "FP64-built opL/opN tables rounded to FP32 (folded by the evenness of k^2 in ky, kz)"
     if var_z == 1:
         return "FP64-built opL/opN radial tables rounded to FP32"
@@ -184,11 +184,11 @@ def operator_source(var_z):
 def z_table_bytes(var_z, n, t, st):
     """HBM bytes of operator tables one z update reads: t per-mode tables for
     the table variants (0, 2); the folded tables, (M+1)(N/2+1)^2 modes read once
-    per step (tiles walked in (ky, N - ky) pairs), for 6-8; none for the radial
+    per step (tiles walked in (ky, N - ky) pairs), for 6-9; none for the radial
     (L2-resident) and computed variants."""
     if var_z in (0, 2):
         return (n // 2 + 1) * n * n * t * st
-    if var_z in (6, 7, 8):
+    if var_z in (6, 7, 8, 9):
         return (n // 2 + 1) * (n // 2 + 1) * (n // 2 + 1) * t * st
     return 0
 
@@ -456,7 +456,7 @@ def run_filtered(args):
     prof = m.profile_step(reps=max(2, args.profile_reps // 2))
     var_z = m.variants()[2]
     tab = {0: 3 * nc * 4, 2: 3 * nc * 4}.get(var_z, 0)
-    if var_z in (6, 7, 8):
+    if var_z in (6, 7, 8, 9):
         tab = 3 * 4 * (shape[0] // 2 + 1) * (shape[1] // 2 + 1) * (shape[2] // 2 + 1)
     ab = {"y_inverse": 16 * nc, "x_fused": 16 * nc, "y_forward": 16 * nc,
           "z_update": nc * 32 + tab, "hermitian_fix": 4 * 2 * shape[1] * shape[2] * 8}
@@ -634,25 +634,26 @@ def run_adjoint(args):
 
 
 def run_axes(args):
-    """Plain batched transforms along y and along z on a --n cube, FP32 (in
-    place along y; z from A into psi_hat): the same TMA-fed column kernel on
-    both axes, so the gap between them is the cost of the axis's stride (kz
-    rows are one kz plane apart: 4 MB at 1024^3).  10 launches per region after
-    --warmup launches, median of --repeats regions; 16 B of traffic per mode."""
+    """Plain batched transforms along y and along z on a --n cube (or --shape),
+    FP32 (in place along y; z from A into psi_hat): the same TMA-fed column
+    kernel on both axes, so the gap between them is the cost of the axis's row
+    stride (kz rows are one kz plane apart: 4 MB at 1024^3).  10 launches per
+    region after --warmup launches, median of --repeats regions; 16 B of traffic
+    per mode."""
     import torch
     import openpfc_b200 as ob
     from openpfc_b200._lib import lib
-    n = N
-    m = ob.PfcB200((n, n, n), DX, r=R, precision=ob.FP32)
+    shape = tuple(args.shape) if args.shape else (N, N, N)
+    m = ob.PfcB200(shape, DX, r=R, precision=ob.FP32)
     m.initialize(DT)
     tune = None if args.no_autotune else m.autotune()
-    psi = torch.full((n, n, n), N0, dtype=torch.float32, device="cuda")
+    psi = torch.full((shape[2], shape[1], shape[0]), N0, dtype=torch.float32, device="cuda")
     psi += AMP * torch.rand_like(psi)
     m.set_psi(psi)
     m.sync()
     del psi
     stream = torch.cuda.ExternalStream(m.stream)
-    nc = (n // 2 + 1) * n * n
+    nc = (shape[0] // 2 + 1) * shape[1] * shape[2]
     hbm, kind = peaks()
     out = {}
     for name, p in (("y_forward", 2), ("z_forward", 6)):
@@ -672,10 +673,11 @@ def run_axes(args):
         ms = statistics.median(regions)
         gbs = 16 * nc / (ms / 1e3) / 1e9
         out[name] = {"ms": ms, "gbs": gbs, "frac": gbs / hbm}
-    line = {"metric": f"plain y and z transforms, {n}^3 FP32 (GB/s on 16 B per mode)", "unit": "GB/s",
+    line = {"metric": f"plain y and z transforms, {'x'.join(map(str, shape))} FP32 (GB/s on 16 B per mode)",
+            "unit": "GB/s",
             "value": out["z_forward"]["gbs"], "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic", "peak": hbm, "peak_kind": kind, "axes": out,
-            "kz_row_stride_bytes": (n // 2) * n * 8, "variants_yxz": m.variants(),
+            "kz_row_stride_bytes": (shape[0] // 2) * shape[1] * 8, "variants_yxz": m.variants(),
             "autotune": tune is not None}
     print(json.dumps(line), flush=True)
     return 0
@@ -709,7 +711,8 @@ def main(argv=None):
                          "calibration (200 steps, snapshots every 20); axes: plain y and z transforms "
                          "of an --n cube")
     ap.add_argument("--shape", type=int, nargs=3, default=None, metavar=("N0", "N1", "N2"),
-                    help="filtered workload only: a non-cubic grid (for profiling one pass on a small case)")
+                    help="filtered and axes workloads: a non-cubic grid (filtered: for profiling one pass "
+                         "on a small case)")
     ap.add_argument("--dry-run", action="store_true",
                     help="launch the ranks and print the line without GPU work (gloo; for tests)")
     args = ap.parse_args(argv)

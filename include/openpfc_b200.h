@@ -242,8 +242,10 @@ const char *opfc_step_kernel_region(int k);
  * from k^2 | 4 direct with computed operators | 5 as 3 with ping-pong exchange
  * buffers (3-5: PLAIN and FILTERED) | 6 pipelined with the folded tables and
  * ping-pong exchange buffers | 7 direct with the folded tables | 8 pipelined
- * with the folded tables (6-8: every model but the moving-gradient Aluminum
- * and caller-supplied operators);
+ * with the folded tables | 9 pipelined with the folded tables and 128-byte
+ * tile rows, the tiles streamed in 256-row boxes through a two-slot ring (z
+ * length 1024, PLAIN and FILTERED; otherwise as 7) (6-9: every model but the
+ * moving-gradient Aluminum and caller-supplied operators);
  * 3 warm-up + 10 timed launches each), keeps the fastest and caches it per
  * device; opfc_initialize applies cached choices.  Every table variant holds
  * operators built in FP64 on the host and rounded once to the compute
@@ -252,10 +254,10 @@ const char *opfc_step_kernel_region(int k);
  * evaluate them per mode in the compute precision, so FP32 handles consider
  * them only with OPFC_FP32_COMPUTED_OPERATORS=1 in the environment.
  * ms (OPFC_AUTOTUNE_SLOTS doubles, may be NULL) receives the mean
- * milliseconds per launch of y0 .. y4 x0 .. x4 z0 .. z8 (-1 if not applicable).
+ * milliseconds per launch of y0 .. y4 x0 .. x4 z0 .. z9 (-1 if not applicable).
  * Call after opfc_initialize; the passes run in place, so set the field
  * afterwards.  opfc_variants reports the chosen (y, x, z) variants. */
-#define OPFC_AUTOTUNE_SLOTS 19
+#define OPFC_AUTOTUNE_SLOTS 20
 int opfc_autotune(opfc_handle *h, double *ms);
 int opfc_variants(const opfc_handle *h, int *var);
 

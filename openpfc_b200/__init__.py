@@ -233,7 +233,7 @@ class _ModelBase(_Handle):
                  "x.no_square",
                  "x.square_direct", "x.square_direct_prefetch",
                  "z.tables", "z.radial", "z.direct", "z.computed", "z.direct_computed", "z.computed_pingpong",
-                 "z.folded_pingpong", "z.direct_folded", "z.folded"]
+                 "z.folded_pingpong", "z.direct_folded", "z.folded", "z.folded_wide"]
         ms = (ctypes.c_double * len(names))()
         _check(self._h, lib().opfc_autotune(self._h, ms))
         return dict(zip(names, list(ms)))

@@ -422,4 +422,171 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Box-ring fused z update with 128-byte tile rows (folded tables, N = 1024).
+//
+// Along z the rows of a column are one kz plane apart (4 MB at 1024^3 FP32), so
+// each row of a tile is its own address translation and the bytes a row brings
+// set the bandwidth: 64-byte rows (the ring kernel above, whose A + psi_hat +
+// table stages do not fit twice at 128-byte rows) hold a plain z transform to
+// ~2.5 TB/s at 1024^3, 128-byte rows reach 4-4.8 TB/s.  This kernel keeps
+// tiles of W = Width<Real>::W columns (128-byte rows) and streams them through
+// shared memory in boxes of 256 rows: per tile A boxes 0..3, then psi_hat boxes
+// 0..3, through a ring of two 32 KB slots, the next box issued as soon as a
+// slot is read; the transforms exchange through their own buffer.  32 values
+// per thread (one exchange per transform): box b holds values 8b .. 8b+7 of
+// every thread.  Operators from the folded tables through L2 (issued before
+// the box they combine with is waited for).  Main segment only; the Nyquist
+// plane runs as a separate direct-load launch.  Bounded waits as in
+// col_tma_kernel (timeout bit 2 of `flag`).
+// ---------------------------------------------------------------------------
+template <typename Real, int N> struct RingCfg {
+  using C = typename Cx<Real>::T;
+  static constexpr int W = 128 / int(sizeof(C));
+  static constexpr int E = 32;
+  static constexpr int T = N / E;
+  static constexpr int NT = W * T;
+  static constexpr int RB = 256;                  // rows per box
+  static constexpr int NB = N / RB;               // boxes per operand
+  static constexpr int VB = RB / T;               // values per thread per box
+  static constexpr size_t BOX = size_t(RB) * W * sizeof(C);
+  static constexpr int LD = W + 1;                // exchange pitch
+  static constexpr size_t TW = align128(size_t(N) * sizeof(C));
+  static constexpr size_t XB = align128(size_t(N) * LD * sizeof(C));
+  static constexpr size_t SLOTS = TW + XB;
+  static constexpr size_t BARS = SLOTS + 2 * BOX;
+  static constexpr size_t SMEM = BARS + 64;
+  static constexpr bool FITS = SMEM <= size_t(kMaxDynSmem) && N % RB == 0 && RB % T == 0 && VB * NB == E;
+};
+
+template <typename Real, int N, int MODEL>
+__global__ void __launch_bounds__(RingCfg<Real, N>::NT, 1)
+    col_ring_kernel(const __grid_constant__ CUtensorMap mA, const __grid_constant__ CUtensorMap mP,
+                    const ColArgs<Real> a, unsigned *flag) {
+  using Cfg = RingCfg<Real, N>;
+  using C = typename Cx<Real>::T;
+  constexpr int W = Cfg::W, E = Cfg::E, T = Cfg::T, NT = Cfg::NT, VB = Cfg::VB, NB = Cfg::NB;
+  constexpr bool CHI = MODEL != MK_PLAIN;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  C *tw = reinterpret_cast<C *>(smraw);
+  C *xb = reinterpret_cast<C *>(smraw + Cfg::TW);
+  unsigned char *slot_b = smraw + Cfg::SLOTS;
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smraw + Cfg::BARS);
+
+  const int tid = threadIdx.x;
+  const int c = tid % W;
+  const int j = tid / W;
+  const C *gtw = reinterpret_cast<const C *>(a.tw);
+  for (int i = tid; i < N; i += NT) tw[i] = gtw[i];
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+
+  const ColSeg sg = a.seg0;
+  const int ntm = sg.ntiles;
+  const int G = gridDim.x;
+  const int nout = sg.tiles_inner > 0 ? ntm / sg.tiles_inner : 0;
+  const int mine = (int)blockIdx.x < ntm ? (ntm - (int)blockIdx.x + G - 1) / G : 0;
+  const int nq = mine * 2 * NB;  // boxes this CTA consumes
+  // box q: tile blockIdx.x + (q / 2NB) G, A box (q % 2NB) or psi_hat box (q % 2NB - NB)
+  auto issue = [&](int q) {
+    const int t = (int)blockIdx.x + (q / (2 * NB)) * G;
+    const int k = q % (2 * NB);
+    const int ti = t % sg.tiles_inner, to = paired_outer(t / sg.tiles_inner, nout);
+    uint64_t *bar = &bars[q & 1];
+    mbar_expect_tx(bar, (unsigned)Cfg::BOX);
+    tma_load_3d(slot_b + size_t(q & 1) * Cfg::BOX, k < NB ? &mA : &mP, bar, ti * W * 2, to, (k % NB) * Cfg::RB);
+  };
+  int qn = 0, qc = 0;  // next box to issue / to consume (the same on every thread)
+  if (tid == 0)
+    for (int q = 0; q < 2 && q < nq; ++q) issue(q);
+  qn = nq < 2 ? nq : 2;
+  bool alive = true;
+  // wait for box qc; false (and the CTA leaves the loop) when the wait expires
+  auto take = [&]() -> const C * {
+    if (!__syncthreads_and(mbar_wait(&bars[qc & 1], (unsigned)(qc >> 1) & 1u))) return nullptr;
+    return reinterpret_cast<const C *>(slot_b + size_t(qc & 1) * Cfg::BOX);
+  };
+  // box qc was read by every thread: refill its slot with box qc + 2
+  auto release = [&]() {
+    fence_proxy_async();
+    __syncthreads();
+    if (qn < nq) {
+      if (tid == 0) issue(qn);
+      ++qn;
+    }
+    ++qc;
+  };
+
+  C *ph = reinterpret_cast<C *>(a.psi_hat);
+  C *gout = reinterpret_cast<C *>(a.out[0]);
+  for (int t = blockIdx.x; t < ntm && alive; t += G) {
+    const int ti = t % sg.tiles_inner, to = paired_outer(t / sg.tiles_inner, nout);
+    const int kx = ti * W + c;
+    const long long base = sg.off + (long long)to * sg.s_outer + (long long)kx * sg.col_stride;
+    const long long fs = sg.fft_stride;
+    C v[E];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      const C *bx = take();
+      if (!bx) {
+        alive = false;
+        break;
+      }
+#pragma unroll
+      for (int u = 0; u < VB; ++u) v[b * VB + u] = bx[(j + T * u) * W + c];
+      release();
+    }
+    if (!alive) break;
+    fft_line_e<C, N, -1, N, E>(v, xb, Cfg::LD, c, j, tw);
+    C w[CHI ? E : 1];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+      // this box's operators first: their L2 round trip overlaps the wait
+      Real la[VB], lb[VB], ch[VB];
+#pragma unroll
+      for (int u = 0; u < VB; ++u) folded_ops<Real, MODEL>(a, kx, to, j + T * (b * VB + u), la[u], lb[u], ch[u]);
+      const C *bx = take();
+      if (!bx) {
+        alive = false;
+        break;
+      }
+#pragma unroll
+      for (int u = 0; u < VB; ++u) {
+        const int m = b * VB + u;
+        const C p = bx[(j + T * u) * W + c];
+        const C np = mk<C>(la[u] * p.x + lb[u] * v[m].x, la[u] * p.y + lb[u] * v[m].y);
+        ph[base + (long long)(j + T * m) * fs] = np;
+        if constexpr (CHI) w[m] = cscale(np, ch[u]);
+        v[m] = np;
+      }
+      release();
+    }
+    if (!alive) break;
+    if constexpr (MODEL == MK_FILTERED) {
+      fft_line_e<C, N, +1, N, E>(w, xb, Cfg::LD, c, j, tw);
+#pragma unroll
+      for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = w[m];
+    } else {
+      fft_line_e<C, N, +1, N, E>(v, xb, Cfg::LD, c, j, tw);
+#pragma unroll
+      for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
+      if constexpr (MODEL == MK_TUNGSTEN) {
+        C *gout2 = reinterpret_cast<C *>(a.out[1]);
+        fft_line_e<C, N, +1, N, E>(w, xb, Cfg::LD, c, j, tw);
+#pragma unroll
+        for (int m = 0; m < E; ++m) gout2[base + (long long)(j + T * m) * fs] = w[m];
+      }
+    }
+  }
+  if (!alive) {
+    if (tid == 0) atomicOr(flag, 2u);
+    // drain this CTA's boxes still in flight (at most two; bounded)
+    for (int k = qc; k < qn; ++k) mbar_wait(&bars[k & 1], (unsigned)(k >> 1) & 1u);
+  }
+}
+
 }  // namespace opfc

@@ -741,8 +741,52 @@ static int launch_col_tma(const ColLaunch &L, cudaStream_t s) {
   }
 }
 
+// Box-ring update with 128-byte rows (N = 1024, folded tables, PLAIN and
+// FILTERED; tensor maps built for Width<Real>::W columns) on the main segment,
+// then the Nyquist plane with the direct-load kernel.  -1 when it does not apply.
+template <typename Real, int N, int MODEL>
+static int launch_col_ring(const ColLaunch &L, cudaStream_t s) {
+  if constexpr (N != 1024 || (MODEL != MK_PLAIN && MODEL != MK_FILTERED)) {
+    return -1;
+  } else {
+    using Cfg = RingCfg<Real, N>;
+    static_assert(Cfg::FITS, "box ring: shared memory and box shape");
+    static_assert(Cfg::W == Width<Real>::W, "128-byte rows are the direct kernels' tile width");
+    if (!L.fold_ops || !L.tmap[0] || !L.tmap[1]) return -1;
+    if (L.seg[0].ncols % Cfg::W != 0 || L.seg[0].col_stride != 1) return -1;
+    auto k = col_ring_kernel<Real, N, MODEL>;
+    static int setup[kDevCache];
+    kernel_setup(k, Cfg::NT, Cfg::SMEM, setup);
+    ColArgs<Real> a = col_args<Real>(L);
+    a.seg1 = ColSeg{};
+    int G = L.num_sms > 0 ? L.num_sms : 148;
+    if (G > a.seg0.ntiles) G = a.seg0.ntiles;
+    if (G >= 1) {
+      k<<<G, Cfg::NT, Cfg::SMEM, s>>>(*reinterpret_cast<const CUtensorMap *>(L.tmap[0]),
+                                     *reinterpret_cast<const CUtensorMap *>(L.tmap[1]), a, L.flag);
+      const int rc = (int)cudaGetLastError();
+      if (rc) return rc;
+    }
+    if (L.nseg < 2 || L.seg[1].ntiles == 0) return 0;
+    // the Nyquist plane: every tile of the direct kernel's launch is a segment-1 tile
+    ColLaunch Ln = L;
+    Ln.seg[0].ntiles = 0;
+    return launch_col_direct<Real, N, COL_UPDATE, -1, MODEL, true, OPS_FOLDED>(Ln, s);
+  }
+}
+
 template <typename Real, int N, int MODE, int DIR, int MODEL, bool INV>
 static int launch_col_t(const ColLaunch &L, cudaStream_t s) {
+  if constexpr (MODE == COL_UPDATE && INV && MODEL != MK_ALUMINUM_G) {
+    if (L.wide && L.fold_ops) {
+      if (L.tmap[0]) {
+        const int rc = launch_col_ring<Real, N, MODEL>(L, s);
+        if (rc >= 0) return rc;
+      }
+      // the tensor maps were built for the ring kernel's width: direct loads
+      return launch_col_direct<Real, N, MODE, DIR, MODEL, INV, OPS_FOLDED>(L, s);
+    }
+  }
   if (L.tmap[0]) {
     int rc;
     if constexpr (MODE == COL_UPDATE)

@@ -82,6 +82,9 @@ struct ColLaunch {
   // COL_PLAIN direct-load kernel with 32 values per thread (N = 512, 1024:
   // one exchange per transform)
   int e32;
+  // COL_UPDATE with the folded tables at N = 1024: the box-ring kernel with
+  // 128-byte tile rows (tensor maps built for Width<Real>::W columns)
+  int wide;
   int axis;            // 1 = y, 2 = z
   unsigned int *flag;  // bit 1: a bounded wait expired
   int num_sms;

@@ -39,10 +39,10 @@ int opfc_scale_by_table(opfc_handle *h, const void *in, const void *tab, void *o
 namespace {
 
 constexpr double kPi = 3.14159265358979323846264338327950288;
-constexpr int kVarY = 5, kVarX = 5, kVarZ = 9;
+constexpr int kVarY = 5, kVarX = 5, kVarZ = 10;
 // z-update variants by how they obtain opL / opN
 inline bool z_computed(int v) { return v >= 3 && v <= 5; }  // from k^2 in the compute precision
-inline bool z_folded(int v) { return v >= 6 && v <= 8; }    // folded FP64-built tables
+inline bool z_folded(int v) { return v >= 6 && v <= 9; }    // folded FP64-built tables
 inline bool z_direct(int v) { return v == 2 || v == 4 || v == 7; }
 // OPFC_FP32_COMPUTED_OPERATORS=1 lets FP32 handles use (and tune) the update
 // variants that compute opL / opN per mode in FP32 (expm1f, fast divide)
@@ -178,7 +178,9 @@ struct opfc_handle {
   //        4 direct with computed operators, 5 as 3 with ping-pong exchange
   //        buffers (3-5: PLAIN and FILTERED), 6 pipelined with the folded
   //        tables and ping-pong exchange buffers, 7 direct with the folded
-  //        tables, 8 pipelined with the folded tables
+  //        tables, 8 pipelined with the folded tables, 9 box-ring kernel with
+  //        the folded tables and 128-byte rows (z length 1024, PLAIN and
+  //        FILTERED; else as 7)
   int var_y = 0, var_x = 0, var_z = 0;
   int num_sms = 148;
   struct Tmap {
@@ -624,7 +626,9 @@ int enqueue_step_kernels(opfc_handle *h, int only) {
     Z.op_r = h->desc.r;
     Z.op_dt = h->dt;
     Z.op_chi = model == OPFC_MODEL_FILTERED ? 1.0 / (2.0 * h->desc.filter_alpha * h->desc.filter_alpha) : 0.0;
-    const int W = tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE);
+    // variant 9: 128-byte rows (the box-ring kernel's tensor maps)
+    Z.wide = h->var_z == 9 && Z.fold_ops && !h->al_grad;
+    const int W = Z.wide ? 128 / (2 * (int)h->rsz) : tma_col_width(Z.N, 2 * (int)h->rsz, COL_UPDATE);
     if (h->use_tma && !h->al_grad && !z_direct(h->var_z) && Z.N > 1 && h->M % W == 0) {
       Z.tmap[0] = tmap_for(h, h->work_a, 2, W, false);
       Z.tmap[1] = tmap_for(h, h->psi_hat, 2, W, false);

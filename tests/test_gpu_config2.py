@@ -7,7 +7,8 @@ Each size runs with the kernel variants the autotuner picks on this GPU and
 with variant sets forced through OPFC_{Y,X,Z}_VARIANT: the ping-pong y pass
 (3), the register-loaded x pass (3) and the z update on the folded FP64-built
 tables (6, 8: the FP32 candidates by default, 8 with the x pass prefetching the
-next row, 4) or on FP32-computed operators (5, an opt-in).  At these sizes every persistent CTA walks many tiles, and the y pass
+next row, 4; 9: the 128-byte-row variant, which at these z lengths takes the
+direct-load kernel) or on FP32-computed operators (5, an opt-in).  At these sizes every persistent CTA walks many tiles, and the y pass
 has 512-point lines.  Tolerances: relative L2 over all cells <= 1e-11 (FP64),
 <= 1e-5 (FP32).
 """
@@ -28,6 +29,7 @@ VARIANTS = {
     "y3x3z6": {"OPFC_Y_VARIANT": "3", "OPFC_X_VARIANT": "3", "OPFC_Z_VARIANT": "6"},
     "y3x3z5": {"OPFC_Y_VARIANT": "3", "OPFC_X_VARIANT": "3", "OPFC_Z_VARIANT": "5"},
     "y3x4z8": {"OPFC_Y_VARIANT": "3", "OPFC_X_VARIANT": "4", "OPFC_Z_VARIANT": "8"},
+    "y3x4z9": {"OPFC_Y_VARIANT": "3", "OPFC_X_VARIANT": "4", "OPFC_Z_VARIANT": "9"},
 }
 
 

@@ -15,7 +15,7 @@ PI4 = [math.pi / 4] * 3
 
 
 @pytest.fixture(params=["tma", "tma_radial", "direct", "computed", "direct_computed", "pingpong", "e32",
-                        "folded", "folded_direct", "folded_nopp"])
+                        "folded", "folded_direct", "folded_nopp", "folded_wide"])
 def path(request, monkeypatch):
     """tma: pipelined kernels streaming the per-mode tables (default);
     tma_radial: the z update reading radial operator tables (OPFC_Z_VARIANT=1,
@@ -36,7 +36,10 @@ def path(request, monkeypatch):
     folded_direct: direct-load z update on the folded tables (OPFC_Z_VARIANT=7);
     folded_nopp: pipelined z update on the folded tables without ping-pong
     buffers (OPFC_Z_VARIANT=8) with the register-loaded x pass prefetching the
-    next row (OPFC_X_VARIANT=4).
+    next row (OPFC_X_VARIANT=4);
+    folded_wide: the z update on the folded tables with 128-byte tile rows
+    streamed through a two-slot box ring (OPFC_Z_VARIANT=9; z lengths other
+    than 1024 and the Tungsten model take the direct-load kernel).
     The Tungsten model has no computed operators and falls back to tables."""
     monkeypatch.delenv("OPFC_NO_TMA", raising=False)
     monkeypatch.delenv("OPFC_Z_VARIANT", raising=False)
@@ -68,6 +71,8 @@ def path(request, monkeypatch):
     elif request.param == "folded_nopp":
         monkeypatch.setenv("OPFC_Z_VARIANT", "8")
         monkeypatch.setenv("OPFC_X_VARIANT", "4")
+    elif request.param == "folded_wide":
+        monkeypatch.setenv("OPFC_Z_VARIANT", "9")
     return request.param
 
 
@@ -77,7 +82,7 @@ def rel_l2(a, b):
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
 @pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 256), (256, 16, 512), (512, 32, 16), (1024, 16, 16),
-                               (16, 512, 512), (32, 128, 128)])
+                               (16, 512, 512), (32, 128, 128), (32, 16, 1024)])
 def test_plain(oracle, path, prec, tol, n):
     psi0 = oracle.ic_noise(n, -0.285, 0.01, 3)
     ref = oracle.run_plain(psi0, PI4, -0.25, 0.5, 10)
@@ -90,7 +95,7 @@ def test_plain(oracle, path, prec, tol, n):
 
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
-@pytest.mark.parametrize("n", [(64, 64, 32), (512, 16, 16), (128, 32, 32), (1024, 16, 8)])
+@pytest.mark.parametrize("n", [(64, 64, 32), (512, 16, 16), (128, 32, 32), (1024, 16, 8), (16, 32, 1024)])
 def test_filtered(oracle, path, prec, tol, n):
     psi0 = oracle.ic_seeds(n, PI4, -0.10, 0.001, 2, 8.0, 0.2, 4)
     ref = oracle.run_filtered(psi0, PI4, -0.3, 0.5, -0.1, -0.5, 0.3, 0.5, 10)
@@ -103,7 +108,7 @@ def test_filtered(oracle, path, prec, tol, n):
 
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
-@pytest.mark.parametrize("n", [(64, 64, 64), (128, 64, 32), (512, 16, 32)])
+@pytest.mark.parametrize("n", [(64, 64, 64), (128, 64, 32), (512, 16, 32), (32, 16, 1024)])
 def test_tungsten(oracle, path, prec, tol, n):
     dx = 1.1107207345395915
     psi0 = np.full((n[2], n[1], n[0]), -0.4)
