@@ -528,6 +528,11 @@ __global__ void __launch_bounds__(RingCfg<Real, N>::NT, 1)
     const int kx = ti * W + c;
     const long long base = sg.off + (long long)to * sg.s_outer + (long long)kx * sg.col_stride;
     const long long fs = sg.fft_stride;
+    // this thread's rows j + T m of the column: pcol[m * rs] (the launcher
+    // checks that N * fs fits a 32-bit offset)
+    const int rs = T * (int)fs;
+    C *pcol = ph + base + (long long)j * fs;
+    C *ocol = gout + base + (long long)j * fs;
     C v[E];
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
@@ -546,9 +551,10 @@ __global__ void __launch_bounds__(RingCfg<Real, N>::NT, 1)
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
       // this box's operators first: their L2 round trip overlaps the wait
-      Real la[VB], lb[VB], ch[VB];
+      // (the filter values, needed last, are loaded after it)
+      C ops[VB];
 #pragma unroll
-      for (int u = 0; u < VB; ++u) folded_ops<Real, MODEL>(a, kx, to, j + T * (b * VB + u), la[u], lb[u], ch[u]);
+      for (int u = 0; u < VB; ++u) ops[u] = __ldg(reinterpret_cast<const C *>(a.fold_ops) + fold_at(a, kx, to, j + T * (b * VB + u)));
       const C *bx = take();
       if (!bx) {
         alive = false;
@@ -558,9 +564,9 @@ __global__ void __launch_bounds__(RingCfg<Real, N>::NT, 1)
       for (int u = 0; u < VB; ++u) {
         const int m = b * VB + u;
         const C p = bx[(j + T * u) * W + c];
-        const C np = mk<C>(la[u] * p.x + lb[u] * v[m].x, la[u] * p.y + lb[u] * v[m].y);
-        ph[base + (long long)(j + T * m) * fs] = np;
-        if constexpr (CHI) w[m] = cscale(np, ch[u]);
+        const C np = mk<C>(ops[u].x * p.x + ops[u].y * v[m].x, ops[u].x * p.y + ops[u].y * v[m].y);
+        pcol[m * rs] = np;
+        if constexpr (CHI) w[m] = cscale(np, __ldg(a.fold_chi + fold_at(a, kx, to, j + T * m)));
         v[m] = np;
       }
       release();
@@ -569,16 +575,16 @@ __global__ void __launch_bounds__(RingCfg<Real, N>::NT, 1)
     if constexpr (MODEL == MK_FILTERED) {
       fft_line_e<C, N, +1, N, E>(w, xb, Cfg::LD, c, j, tw);
 #pragma unroll
-      for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = w[m];
+      for (int m = 0; m < E; ++m) ocol[m * rs] = w[m];
     } else {
       fft_line_e<C, N, +1, N, E>(v, xb, Cfg::LD, c, j, tw);
 #pragma unroll
-      for (int m = 0; m < E; ++m) gout[base + (long long)(j + T * m) * fs] = v[m];
+      for (int m = 0; m < E; ++m) ocol[m * rs] = v[m];
       if constexpr (MODEL == MK_TUNGSTEN) {
         C *gout2 = reinterpret_cast<C *>(a.out[1]);
         fft_line_e<C, N, +1, N, E>(w, xb, Cfg::LD, c, j, tw);
 #pragma unroll
-        for (int m = 0; m < E; ++m) gout2[base + (long long)(j + T * m) * fs] = w[m];
+        for (int m = 0; m < E; ++m) gout2[base + (long long)j * fs + m * rs] = w[m];
       }
     }
   }

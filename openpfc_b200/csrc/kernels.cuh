@@ -54,14 +54,20 @@ enum OpsKind { OPS_TABLES = 0, OPS_RADIAL = 1, OPS_COMPUTED = 2, OPS_FOLDED = 3 
 // the same k^2, so every operator of k^2 is even in it)
 __device__ __forceinline__ int fold_index(int i, int n) { return i <= n / 2 ? i : n - i; }
 
+// Index of mode (kx, ky, kz) in the folded tables.
+template <typename Real>
+__device__ __forceinline__ long long fold_at(const ColArgs<Real> &a, int kx, int ky, int kz) {
+  const long long r =
+      (long long)fold_index(ky, a.rad_n1) + (long long)(a.rad_n1 / 2 + 1) * fold_index(kz, a.rad_n2);
+  return kx < a.rad_M ? kx + (long long)a.rad_M * r : a.fold_nyq + r;
+}
+
 // Operators of mode (kx, ky, kz) read from the folded tables (direct loads).
 template <typename Real, int MODEL>
 __device__ __forceinline__ void folded_ops(const ColArgs<Real> &a, int kx, int ky, int kz, Real &la, Real &lb,
                                            Real &ch) {
   using C = typename Cx<Real>::T;
-  const long long r =
-      (long long)fold_index(ky, a.rad_n1) + (long long)(a.rad_n1 / 2 + 1) * fold_index(kz, a.rad_n2);
-  const long long i = kx < a.rad_M ? kx + (long long)a.rad_M * r : a.fold_nyq + r;
+  const long long i = fold_at(a, kx, ky, kz);
   const C o = __ldg(reinterpret_cast<const C *>(a.fold_ops) + i);
   la = o.x;
   lb = o.y;
@@ -754,6 +760,7 @@ static int launch_col_ring(const ColLaunch &L, cudaStream_t s) {
     static_assert(Cfg::W == Width<Real>::W, "128-byte rows are the direct kernels' tile width");
     if (!L.fold_ops || !L.tmap[0] || !L.tmap[1]) return -1;
     if (L.seg[0].ncols % Cfg::W != 0 || L.seg[0].col_stride != 1) return -1;
+    if ((long long)N * L.seg[0].fft_stride >= (1ll << 31)) return -1;  // in-column offsets are 32-bit
     auto k = col_ring_kernel<Real, N, MODEL>;
     static int setup[kDevCache];
     kernel_setup(k, Cfg::NT, Cfg::SMEM, setup);
