@@ -1665,7 +1665,16 @@ size_t opfc_size_outbox(const opfc_handle *h) { return h ? h->nc : 0; }
 size_t opfc_allocated_bytes(const opfc_handle *h) { return h ? h->allocated : 0; }
 void *opfc_get_stream(const opfc_handle *h) { return h ? (void *)h->stream : nullptr; }
 // (the Aluminum gradient model's y pass launches once more, for P*psi)
-int opfc_kernels_per_step(const opfc_handle *h) { return h ? kStepKernels + (h->al_grad ? 1 : 0) : 0; }
+// (the box-ring z update of z variant 9 launches once more, for the Nyquist
+// plane, where it applies: z length 1024, PLAIN or FILTERED, TMA-fed passes)
+int opfc_kernels_per_step(const opfc_handle *h) {
+  if (!h) return 0;
+  const int model = h->desc.model;
+  const bool ring = h->var_z == 9 && h->n2 == 1024 && h->fold_ops && h->use_tma && !h->al_grad &&
+                    (model == OPFC_MODEL_PLAIN || model == OPFC_MODEL_FILTERED) &&
+                    h->M % (128 / (2 * (int)h->rsz)) == 0;
+  return kStepKernels + (h->al_grad ? 1 : 0) + (ring ? 1 : 0);
+}
 
 int opfc_autotune(opfc_handle *h, double *ms) {
   if (!h) return OPFC_ERR_ARG;
