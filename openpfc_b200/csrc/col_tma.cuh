@@ -435,8 +435,9 @@ __global__ void __launch_bounds__(W *(N / Plan<N>::E), MINB)
 // 0..3, through a ring of two 32 KB slots, the next box issued as soon as a
 // slot is read; the transforms exchange through their own buffer.  32 values
 // per thread (one exchange per transform): box b holds values 8b .. 8b+7 of
-// every thread.  Operators from the folded tables through L2 (issued before
-// the box they combine with is waited for).  Main segment only; the Nyquist
+// every thread.  Operators from the folded tables through L2: a box's (opL,
+// opN) pairs are issued before the box is waited for, the filter values after
+// (fewer live registers).  Main segment only; the Nyquist
 // plane runs as a separate direct-load launch.  Bounded waits as in
 // col_tma_kernel (timeout bit 2 of `flag`).
 // ---------------------------------------------------------------------------
