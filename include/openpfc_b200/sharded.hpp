@@ -34,6 +34,7 @@
 
 #include <array>
 #include <cmath>
+#include <complex>
 #include <numeric>
 #include <stdexcept>
 #include <string>
@@ -273,6 +274,7 @@ template <typename T = float> class ShardedPfc {
   cudaStream_t stream() const { return stream_; }
 
  private:
+  template <typename> friend class ShardedFft;
   static constexpr size_t kCs = 2 * sizeof(T);  // one complex value
   struct Rank {
     int rank = 0;
@@ -399,6 +401,98 @@ template <typename T = float> class ShardedPfc {
   std::vector<std::vector<T>> host_;  // host staging of set_psi / get_psi
   double mean_ = 0.0;
   bool a_ready_ = false;
+};
+
+/// The sharded 3D transform alone, the IFFT contract over a decomposed field
+/// (fft_interface.hpp:51,61 on the decomposition of fft.cpp:72-81): forward
+/// takes each local rank's real z slab (N2/P x N1 x N0, x fastest) and returns
+/// its kx slab of the half spectrum, N2 x N1 x cols complex values in the
+/// reference order, cols = N0/(2P) plus the kx = N0/2 plane on the last rank;
+/// backward is the inverse with the 1/(N0 N1 N2) scaling.
+template <typename T = double> class ShardedFft {
+ public:
+  ShardedFft(std::array<int, 3> n, ShardComm &comm, int device = 0)
+      : m_(n, {1.0, 1.0, 1.0}, comm, ShardedParams(), device) {}
+
+  /// Columns of local rank i's kx slab (reference order, last rank + 1).
+  int columns(size_t i) const { return m_.mloc_ + (m_.ranks_[i].rank == m_.P_ - 1 ? 1 : 0); }
+
+  void forward(const std::vector<const double *> &slabs, const std::vector<std::complex<double> *> &out) {
+    m_.need(slabs.size(), "forward");
+    m_.need(out.size(), "forward");
+    upload_real(slabs);
+    for (auto &R : m_.ranks_) m_.pass(R.zs, OPFC_PASS_XY_FORWARD);
+    m_.z_to_kx();
+    for (auto &R : m_.ranks_) m_.pass(R.kx, OPFC_PASS_Z_FORWARD);
+    const size_t lines = size_t(m_.n_[1]) * m_.n_[2], ml = size_t(m_.mloc_);
+    std::vector<std::vector<T>> h(m_.ranks_.size(), std::vector<T>(2 * (ml + 1) * lines));
+    for (size_t i = 0; i < m_.ranks_.size(); ++i)
+      cuda_check(cudaMemcpyAsync(h[i].data(), opfc_array(m_.ranks_[i].kx, OPFC_ARRAY_STATE),
+                                 h[i].size() * sizeof(T), cudaMemcpyDeviceToHost, m_.stream_),
+                 "ShardedFft::forward");
+    m_.sync();
+    for (size_t i = 0; i < m_.ranks_.size(); ++i) {
+      const size_t cols = size_t(columns(i));
+      const T *main = h[i].data(), *nyq = main + 2 * ml * lines;
+      for (size_t l = 0; l < lines; ++l) {
+        for (size_t k = 0; k < ml; ++k)
+          out[i][l * cols + k] = std::complex<double>(main[2 * (l * ml + k)], main[2 * (l * ml + k) + 1]);
+        if (cols > ml) out[i][l * cols + ml] = std::complex<double>(nyq[2 * l], nyq[2 * l + 1]);
+      }
+    }
+  }
+
+  void backward(const std::vector<const std::complex<double> *> &in, const std::vector<double *> &slabs) {
+    m_.need(in.size(), "backward");
+    m_.need(slabs.size(), "backward");
+    const size_t lines = size_t(m_.n_[1]) * m_.n_[2], ml = size_t(m_.mloc_);
+    std::vector<std::vector<T>> h(m_.ranks_.size(), std::vector<T>(2 * (ml + 1) * lines, T(0)));
+    for (size_t i = 0; i < m_.ranks_.size(); ++i) {
+      const size_t cols = size_t(columns(i));
+      T *main = h[i].data(), *nyq = main + 2 * ml * lines;
+      for (size_t l = 0; l < lines; ++l) {
+        for (size_t k = 0; k < ml; ++k) {
+          main[2 * (l * ml + k)] = T(in[i][l * cols + k].real());
+          main[2 * (l * ml + k) + 1] = T(in[i][l * cols + k].imag());
+        }
+        if (cols > ml) {  // the kx = N0/2 plane lives on the last rank only
+          nyq[2 * l] = T(in[i][l * cols + ml].real());
+          nyq[2 * l + 1] = T(in[i][l * cols + ml].imag());
+        }
+      }
+      cuda_check(cudaMemcpyAsync(opfc_array(m_.ranks_[i].kx, OPFC_ARRAY_STATE), h[i].data(),
+                                 h[i].size() * sizeof(T), cudaMemcpyHostToDevice, m_.stream_),
+                 "ShardedFft::backward");
+    }
+    for (auto &R : m_.ranks_) m_.pass(R.kx, OPFC_PASS_Z_INVERSE_STATE);
+    m_.kx_to_z();
+    for (auto &R : m_.ranks_) m_.pass(R.zs, OPFC_PASS_XY_BACKWARD, 0.0);
+    download_real(slabs);
+  }
+
+ private:
+  void upload_real(const std::vector<const double *> &slabs) {
+    const size_t cells = m_.rows_ * size_t(m_.n_[0]);
+    m_.host_.assign(m_.ranks_.size(), std::vector<T>());
+    for (size_t i = 0; i < m_.ranks_.size(); ++i) {
+      m_.host_[i].assign(slabs[i], slabs[i] + cells);
+      cuda_check(cudaMemcpyAsync(opfc_array(m_.ranks_[i].zs, OPFC_ARRAY_REAL), m_.host_[i].data(),
+                                 cells * sizeof(T), cudaMemcpyHostToDevice, m_.stream_),
+                 "ShardedFft");
+    }
+  }
+  void download_real(const std::vector<double *> &slabs) {
+    const size_t cells = m_.rows_ * size_t(m_.n_[0]);
+    m_.host_.assign(m_.ranks_.size(), std::vector<T>(cells));
+    for (size_t i = 0; i < m_.ranks_.size(); ++i)
+      cuda_check(cudaMemcpyAsync(m_.host_[i].data(), opfc_array(m_.ranks_[i].zs, OPFC_ARRAY_REAL),
+                                 cells * sizeof(T), cudaMemcpyDeviceToHost, m_.stream_),
+                 "ShardedFft");
+    m_.sync();
+    for (size_t i = 0; i < m_.ranks_.size(); ++i)
+      for (size_t c = 0; c < cells; ++c) slabs[i][c] = double(m_.host_[i][c]);
+  }
+  ShardedPfc<T> m_;
 };
 
 }  // namespace b200
