@@ -11,6 +11,8 @@
 //                           -- the on-disk formats (frontend/io/binary_writer.hpp,
 //                              kernel/simulation/binary_reader.hpp, frontend/io/vtk_writer.hpp,
 //                              initial_conditions/file_reader.hpp, frontend/utils/utils.hpp)
+// A field decomposed over ranks (fft.cpp:72-81) is in openpfc_b200/sharded.hpp
+// (ShardedPfc, ShardedFft).
 // Size contracts throw std::invalid_argument, unknown fields std::out_of_range,
 // everything else std::runtime_error (as in the reference).  T selects the
 // device precision (float or double); host fields are std::vector<double>.
