@@ -283,7 +283,7 @@ template <> struct Plan<64> { static constexpr int E = 8; using R = Radices<8, 8
 template <> struct Plan<128> { static constexpr int E = 8; using R = Radices<2, 8, 8>; };
 template <> struct Plan<256> { static constexpr int E = 8; using R = Radices<4, 8, 8>; };
 template <> struct Plan<512> { static constexpr int E = 8; using R = Radices<8, 8, 8>; };
-template <> struct Plan<1024> { static constexpr int E = 16; using R = Radices<2, 8, 8, 8>; };
+template <> struct Plan<1024> { static constexpr int E = 16; using R = Radices<16, 8, 8>; };
 // non power-of-two lengths used by uneven ensembles (x half lengths 24, 40, 48)
 template <> struct Plan<24> { static constexpr int E = 24; using R = Radices<3, 8>; };
 template <> struct Plan<40> { static constexpr int E = 20; using R = Radices<5, 2, 4>; };

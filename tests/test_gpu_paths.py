@@ -82,7 +82,7 @@ def rel_l2(a, b):
 
 @pytest.mark.parametrize("prec,tol", [(ob.FP64, 1e-11), (ob.FP32, 1e-5)])
 @pytest.mark.parametrize("n", [(64, 64, 64), (128, 32, 256), (256, 16, 512), (512, 32, 16), (1024, 16, 16),
-                               (16, 512, 512), (32, 128, 128), (32, 16, 1024)])
+                               (16, 512, 512), (32, 128, 128), (32, 16, 1024), (32, 1024, 16)])
 def test_plain(oracle, path, prec, tol, n):
     psi0 = oracle.ic_noise(n, -0.285, 0.01, 3)
     ref = oracle.run_plain(psi0, PI4, -0.25, 0.5, 10)
